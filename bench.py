@@ -1,0 +1,332 @@
+"""Benchmark of the dbscan2d hot path on B200 (one JSON line on stdout).
+
+Workload: the constant-density cloud at N = 10,000,000 float32 points
+(K = N/5,000 Gaussian blobs, sigma 1, centres uniform in a square of side
+2*sqrt(N)/10, plus 2% uniform noise; eps 0.5, min_samples 10), seeded
+synthetic data. One step = one dbscan2d call over the whole cloud.
+
+  value     Mpoints/s of the pipeline with X resident in HBM (CUDA events on
+            the launching stream around each call; L2 flushed between steps
+            by writing a 512 MB buffer outside the timed events)
+  e2e       same metric through the public API with HOST buffers: a pinned
+            CPU tensor in, CPU labels out (H2D of X and D2H of labels inside
+            the timed region)
+  roofline  dominant stage: algorithmic bytes per launch / its average launch
+            time (per-stage CUDA events of dbscan2d_profile), against the
+            measured HBM copy bandwidth in MEASURED_PEAKS.json
+  cpu_baseline  the reference's own CPU implementation (built from its
+            sources into oracle/_ref/cpu) on the box's host cores, timed on
+            the same workload
+
+--impl reference times only that reference CPU path and prints its line.
+Multi-GPU (torchrun): replicas only -- every rank clusters its own cloud;
+the time is the max over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "dbscan-torch_b200"))
+
+import numpy as np  # noqa: E402
+import torch  # noqa: E402
+
+METRIC = "Mpoints/s @10M"
+UNIT = "Mpoints/s"
+N_POINTS = 10_000_000
+EPS, MIN_SAMPLES = 0.5, 10
+WORKLOAD = "constant_density_10M"
+L2_FLUSH_BYTES = 512 << 20
+KERNELS_PER_CALL = 18  # init, bounds, seg_finalize, keys_hist, 8 onesweep, rle, cell_prep,
+                       # core, union, ids, labels
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([v.strip() for v in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4)
+                          if len(s) > 3 + k and s[3 + k].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons}
+
+
+def stage_bytes(n: int, cells: int, passes: int, kb: int) -> dict:
+    """Algorithmic (compulsory) bytes per stage: each array the stage must
+    touch, counted once (per-point and per-cell figures)."""
+    return {
+        "cell_keys": n * (8 + kb),                                   # read X, write key
+        "sort_gather": n * (passes * (2 * kb + 8) - 4 + 16),         # key+idx per pass, X gather, xy
+        "boundary_scan": n * kb + cells * 16,                        # sorted keys; start, key, seg
+        "build_ngh": n * 8 + cells * (4 + 8 + 16 + 100),             # xy; start, key, bbox, 25 ngh
+        "core_mark": n * (8 + 1) + cells * (100 + 4 + 1 + 4),        # xy, is_core; ngh, start, status, uf
+        "union_find": n * (8 + 1) + cells * (100 + 16 + 1 + 4),      # xy, is_core; ngh, bbox, status, uf
+        "cluster_id": cells * (4 + 1 + 4 + 4),                       # uf r/w, status, rank
+        "core_labels": 0,
+        "border_assign": n * (8 + 1 + 4 + 4) + cells * (100 + 4 + 4),  # xy, is_core, perm, labels
+        "unpermute": 0,
+    }
+
+
+def stage_launches(passes: int) -> dict:
+    return {"cell_keys": 4, "sort_gather": passes, "boundary_scan": 1, "build_ngh": 1,
+            "core_mark": 1, "union_find": 1, "cluster_id": 1, "border_assign": 1}
+
+
+def cpu_baseline(X: np.ndarray, eps: float, ms: int, budget_s: float = 15.0):
+    """The reference's CPU path (oracle/_ref/cpu) on all host cores, else the
+    single-threaded C oracle port; bounded to ~budget_s of CPU work."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import refmod
+    ref = refmod.load("cpu")
+    cores = os.cpu_count() or 1
+    if ref is not None:
+        torch.set_num_threads(cores)
+        Xt = torch.from_numpy(X)
+        ref.dbscan2d(Xt, eps, ms)  # warm-up
+        times = []
+        t_end = time.perf_counter() + budget_s
+        while len(times) < 3 or (time.perf_counter() < t_end and len(times) < 20):
+            t0 = time.perf_counter()
+            ref.dbscan2d(Xt, eps, ms)
+            times.append(time.perf_counter() - t0)
+        kind, used = "reference", torch.get_num_threads()
+    else:
+        import oracle
+        times = []
+        t_end = time.perf_counter() + budget_s
+        while len(times) < 1 or (time.perf_counter() < t_end and len(times) < 5):
+            t0 = time.perf_counter()
+            oracle.dbscan2d(X, eps, ms)
+            times.append(time.perf_counter() - t0)
+        kind, used = "port", 1
+    med = statistics.median(times)
+    return {"value": round(X.shape[0] / med / 1e6, 3), "unit": UNIT, "cores": used, "kind": kind,
+            "sample": f"{len(times)} calls on the full {X.shape[0]:,}-point workload, median "
+                      f"{med * 1e3:.1f} ms/call ({cores} host cores visible)"}
+
+
+def dist_setup(n_gpus: int):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(v: float, world: int) -> float:
+    if world == 1:
+        return v
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def run_reference(args, world, rank):
+    from dbscan_torch import synthetic
+    if rank != 0:
+        return None
+    X = synthetic.constant_density(N_POINTS, seed=0)
+    base = cpu_baseline(X, EPS, MIN_SAMPLES, budget_s=max(10.0, 2.0 * args.steps))
+    return {"metric": METRIC, "value": base["value"], "unit": UNIT, "impl": "reference",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(N_POINTS / (base["value"] * 1e6) * 1e3, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded constant-density Gaussian blobs + 2% noise)",
+            "config": {"workload": WORKLOAD, "n_points": N_POINTS, "eps": EPS,
+                       "min_samples": MIN_SAMPLES, "device": "host CPU"},
+            "cpu_baseline": base,
+            "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+def run_ours(args, world, rank, local):
+    from dbscan_torch import _C, dbscan2d, synthetic
+    dev = torch.device("cuda", local)
+    X_np = synthetic.constant_density(N_POINTS, seed=rank)
+    X = torch.from_numpy(X_np).to(dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    # Shape of the pipeline on this input (cells, key width, passes).
+    _, info = _C.dbscan2d_info(X, EPS, MIN_SAMPLES)
+    for _ in range(max(3, args.warmup)):
+        dbscan2d(X, EPS, MIN_SAMPLES)
+    _C.check_status()
+
+    barrier(world)
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    with ClockSampler(local) as clocks:
+        for k in range(args.steps):
+            flush.fill_(float(k))
+            ev[k][0].record(stream)
+            labels = dbscan2d(X, EPS, MIN_SAMPLES)
+            ev[k][1].record(stream)
+        torch.cuda.synchronize()
+    barrier(world)
+    _C.check_status()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    ms_mean = sum(step_ms) / len(step_ms)
+    ms_max = max_over_ranks(ms_mean, world)
+    value = world * N_POINTS / (ms_max * 1e-3) / 1e6
+
+    # Per-stage split (profile entry point: CUDA events between stages).
+    prof_runs = []
+    for k in range(3):
+        flush.fill_(float(k))
+        _, prof = _C.dbscan2d_profile(X, EPS, MIN_SAMPLES)
+        prof_runs.append(prof)
+    prof = {s: statistics.median(r[s] for r in prof_runs) for s in prof_runs[0]}
+    cells, passes, kb = info["num_cells"], info["passes"], info["key_bytes"]
+    sb = stage_bytes(N_POINTS, cells, passes, kb)
+    launches = stage_launches(passes)
+    dom = max((s for s in launches), key=lambda s: prof[s])
+    peak, peak_kind = _peaks()
+    per_launch_ms = prof[dom] / launches[dom]
+    achieved = sb[dom] / launches[dom] / (per_launch_ms * 1e-3) / 1e9
+    b_alg_total = sum(sb.values())
+    roof = {"bound": "hbm", "kernel": dom, "launches": launches[dom],
+            "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+            "traffic": None,
+            "pipeline_alg_bytes": b_alg_total,
+            "pipeline_frac": round(b_alg_total / (ms_mean * 1e-3) / 1e9 / peak, 4),
+            "stage_ms": {s: round(v, 4) for s, v in prof.items()},
+            "stage_frac": {s: round(sb[s] / (prof[s] * 1e-3) / 1e9 / peak, 4)
+                           for s in launches if prof[s] > 0}}
+    traffic_file = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(traffic_file):
+        try:
+            with open(traffic_file) as f:
+                roof["traffic"] = json.load(f).get(dom)
+        except Exception:
+            pass
+
+    # End to end through the public API with host buffers.
+    X_host = torch.from_numpy(X_np).pin_memory()
+    for _ in range(2):
+        dbscan2d(X_host, EPS, MIN_SAMPLES)
+    e2e_ms = []
+    for k in range(args.steps):
+        flush.fill_(float(k))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        lab_host = dbscan2d(X_host, EPS, MIN_SAMPLES)
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    e2e_mean = max_over_ranks(sum(e2e_ms) / len(e2e_ms), world)
+    assert lab_host.device.type == "cpu"
+
+    out = {"metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max, 4),
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+           "data": "synthetic (seeded constant-density Gaussian blobs + 2% noise)",
+           "config": {"workload": WORKLOAD, "n_points": N_POINTS, "eps": EPS,
+                      "min_samples": MIN_SAMPLES, "parallelism": "replicas" if world > 1 else "single",
+                      "l2": "flushed between steps (512 MB write outside the timed events)",
+                      "num_cells": cells, "key_bits": info["key_bits"], "radix_passes": passes},
+           "clocks": clocks.summary(),
+           "e2e": {"value": round(world * N_POINTS / (e2e_mean * 1e-3) / 1e6, 2), "unit": UNIT,
+                   "h2d_bytes_per_step": N_POINTS * 8, "d2h_bytes_per_step": N_POINTS * 4},
+           "gpu_launches": KERNELS_PER_CALL * args.steps,
+           "roofline": roof}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(X_np, EPS, MIN_SAMPLES)
+    del labels
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_setup(args.gpus)
+    try:
+        if args.impl == "reference":
+            out = run_reference(args, world, rank)
+        else:
+            out = run_ours(args, world, rank, local)
+        if rank == 0 and out is not None:
+            print(json.dumps(out), flush=True)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

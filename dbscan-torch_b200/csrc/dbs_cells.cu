@@ -1,0 +1,203 @@
+// dbs_cells.cu -- run-length cells, per-cell bounding boxes and neighbour table.
+//
+// Reference path replaced (ryanirl/dbscan-torch v0.2.0, csrc/cuda/dbscan_cuda.cu):
+//   k_boundary_flags :84-89, thrust::inclusive_scan :606-609, the host read of
+//   num_cells :612-617 (removed: the count stays on the device),
+//   k_point_cell_from_scan :95-101, k_extract_cell_start :106-120,
+//   k_cell_bbox :162-177, binsearch_cell / k_build_ngh :125-150.
+//
+// k_rle turns the sorted keys into cells with one decoupled look-back scan of
+// the boundary flags (4096 keys per tile). Cells keep the reference's order
+// (ascending unsigned key), so cell indices are the reference's. Dense clouds
+// also record each cell in a dense map indexed by the compacted key, so
+// neighbour lookup is one load instead of a binary search.
+//
+// k_cell_prep gives each cell one warp: the lanes reduce the bounding box of
+// the cell's points and lanes 0..24 resolve the 25 offsets of the 5x5
+// stencil in the reference's order (off = (dx+2)*5 + (dy+2)).
+#include "dbs_internal.cuh"
+
+namespace dbs {
+
+// ------------------------------------------------------------------ k_rle
+template <typename K>
+__device__ __forceinline__ void rle_body(const Plan& p, K* s_keys, uint32_t* s_warp,
+                                         uint32_t* s_tile, unsigned long long* s_excl) {
+  Desc* d = p.desc;
+  const int64_t n = p.n;
+  const K* keys = reinterpret_cast<const K*>(p.keys[d->npasses & 1]);
+  const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
+  const int nwarps = blockDim.x >> 5;
+  while (true) {
+    if (threadIdx.x == 0) *s_tile = atomicAdd(&d->ctr[kCtrRle], 1u);
+    __syncthreads();
+    const int64_t tile = *s_tile;
+    if (tile >= p.scan_tiles) break;
+    const int64_t base = tile * kScanTile;
+    const int32_t valid = (int32_t)min((int64_t)kScanTile, n - base);
+    // Coalesced load into shared memory, then blocked reads.
+    for (int32_t j = threadIdx.x; j < valid; j += blockDim.x) s_keys[j + 1] = keys[base + j];
+    if (threadIdx.x == 0) s_keys[0] = base > 0 ? keys[base - 1] : (K)0;
+    __syncthreads();
+    const int32_t j0 = threadIdx.x * kScanItems;
+    uint32_t flags = 0;
+    uint32_t cnt = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+      const int32_t j = j0 + k;
+      if (j < valid) {
+        const bool f = (base + j == 0) || (s_keys[j + 1] != s_keys[j]);
+        flags |= (uint32_t)f << k;
+        cnt += f;
+      }
+    }
+    // Block exclusive scan of per-thread counts.
+    uint32_t x = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= (uint32_t)o) x += y;
+    }
+    if (lane == 31) s_warp[warp] = x;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint32_t run = 0;
+      for (int w = 0; w < nwarps; ++w) { const uint32_t t = s_warp[w]; s_warp[w] = run; run += t; }
+      unsigned long long* my = p.rle_status + tile;
+      unsigned long long excl = 0;
+      if (tile == 0) st_relaxed(my, kFlagInc | run);
+      else {
+        st_relaxed(my, kFlagAgg | run);
+        excl = lookback(p.rle_status, tile, 1, d);
+        st_relaxed(my, kFlagInc | (excl + run));
+      }
+      *s_excl = excl;
+      if (base + valid == n) {
+        uint32_t total = (uint32_t)(excl + run);
+        if ((int64_t)total > n) total = (uint32_t)n;  // only after a failed look-back
+        d->num_cells = total;
+        p.cell_start[total] = (int32_t)n;
+      }
+    }
+    __syncthreads();
+    uint32_t c = (uint32_t)*s_excl + s_warp[warp] + x - cnt;
+    if (flags) {
+      int32_t seg = seg_of(p, base + j0);
+#pragma unroll 1
+      for (int k = 0; k < kScanItems; ++k) {
+        if (!((flags >> k) & 1u)) continue;
+        const int64_t i = base + j0 + k;
+        const uint64_t key = (uint64_t)s_keys[j0 + k + 1];
+        while (i >= p.seg_off[seg + 1]) ++seg;
+        if ((int64_t)c >= n) break;  // only after a failed look-back
+        p.cell_start[c] = (int32_t)i;
+        p.cell_key[c] = key;
+        p.cell_seg[c] = seg;
+        if (i == p.seg_off[seg]) p.seg_info[seg].cell_begin = (int32_t)c;
+        const int64_t mb = p.seg_info[seg].map_base;
+        if (mb >= 0) p.cell_map[mb + (int64_t)(key - p.seg_info[seg].base)] = (int32_t)c;
+        ++c;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_rle(Plan p) {
+  __shared__ __align__(16) unsigned char s_raw[sizeof(uint64_t) * (kScanTile + 1)];
+  __shared__ uint32_t s_warp[kScanThreads / 32];
+  __shared__ uint32_t s_tile;
+  __shared__ unsigned long long s_excl;
+  if (p.desc->key64)
+    rle_body<uint64_t>(p, reinterpret_cast<uint64_t*>(s_raw), s_warp, &s_tile, &s_excl);
+  else
+    rle_body<uint32_t>(p, reinterpret_cast<uint32_t*>(s_raw), s_warp, &s_tile, &s_excl);
+}
+
+// ------------------------------------------------------------ k_cell_prep
+__device__ __forceinline__ int32_t find_cell(const Plan& p, const SegInfo& g, int32_t s,
+                                             uint64_t gx, uint64_t gy, uint32_t num_cells) {
+  const uint64_t local = gx * g.wy + gy;
+  if (g.map_base >= 0) return p.cell_map[g.map_base + (int64_t)local];
+  const uint64_t target = g.base + local;
+  // Binary search over the cloud's cells (at most min(range, points) cells).
+  const int64_t npts = p.seg_off[s + 1] - p.seg_off[s];
+  int64_t lo = g.cell_begin;
+  int64_t hi = min((int64_t)num_cells, lo + npts);
+  while (lo < hi) {
+    const int64_t mid = (lo + hi) >> 1;
+    if (p.cell_key[mid] < target) lo = mid + 1; else hi = mid;
+  }
+  if (lo < (int64_t)num_cells && p.cell_key[lo] == target) return (int32_t)lo;
+  return -1;
+}
+
+__global__ void __launch_bounds__(kCellThreads) k_cell_prep(Plan p) {
+  const uint32_t full = 0xffffffffu;
+  const uint32_t lane = lane_id();
+  const uint32_t C = p.desc->num_cells;
+  while (true) {
+    uint32_t c = 0;
+    if (lane == 0) c = atomicAdd(&p.desc->ctr[kCtrPrep], 1u);
+    c = __shfl_sync(full, c, 0);
+    if (c >= C) break;
+    const int32_t s0 = p.cell_start[c], s1 = p.cell_start[c + 1];
+    // Bounding box. A one-point cell keeps its raw coordinates (the
+    // reference seeds the fold with xs[s] and folds fminf/fmaxf over the
+    // rest, which flushes subnormals only when there is a rest).
+    float xmin = INFINITY, xmax = -INFINITY, ymin = INFINITY, ymax = -INFINITY;
+    for (int32_t i = s0 + lane; i < s1; i += 32) {
+      const float2 v = p.xy[i];
+      xmin = fminf(xmin, v.x); xmax = fmaxf(xmax, v.x);
+      ymin = fminf(ymin, v.y); ymax = fmaxf(ymax, v.y);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      xmin = fminf(xmin, __shfl_xor_sync(full, xmin, o));
+      xmax = fmaxf(xmax, __shfl_xor_sync(full, xmax, o));
+      ymin = fminf(ymin, __shfl_xor_sync(full, ymin, o));
+      ymax = fmaxf(ymax, __shfl_xor_sync(full, ymax, o));
+    }
+    if (lane == 0) {
+      if (s1 - s0 == 1) {
+        const float2 v = p.xy[s0];
+        p.bbox[c] = make_float4(v.x, v.x, v.y, v.y);
+      } else {
+        p.bbox[c] = make_float4(xmin, xmax, ymin, ymax);
+      }
+    }
+    // Neighbour table.
+    if (lane < kNgh) {
+      const int32_t s = p.cell_seg[c];
+      const SegInfo& g = p.seg_info[s];
+      const uint64_t local = p.cell_key[c] - g.base;
+      const uint64_t gx = local / g.wy;
+      const uint64_t gy = local - gx * g.wy;
+      const int32_t kx = expand_axis(gx, g.bx, g.px);
+      const int32_t ky = expand_axis(gy, g.by, g.py);
+      const int32_t dx = (int32_t)(lane / 5) - 2, dy = (int32_t)(lane % 5) - 2;
+      const int32_t nkx = (int32_t)((uint32_t)kx + (uint32_t)dx);
+      const int32_t nky = (int32_t)((uint32_t)ky + (uint32_t)dy);
+      const uint64_t ngx = compact_axis(nkx, g.bx, g.px);
+      const uint64_t ngy = compact_axis(nky, g.by, g.py);
+      int32_t r = -1;
+      if (ngx != ~0ull && ngy != ~0ull) r = find_cell(p, g, s, ngx, ngy, C);
+      p.ngh[(int64_t)c * kNgh + lane] = r;
+    }
+  }
+}
+
+// ------------------------------------------------------------- launchers
+cudaError_t launch_rle(const Plan& p, cudaStream_t s) {
+  int grid = p.num_sms * 4;
+  if (grid > p.scan_tiles) grid = p.scan_tiles > 0 ? p.scan_tiles : 1;
+  k_rle<<<grid, kScanThreads, 0, s>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_cell_prep(const Plan& p, cudaStream_t s) {
+  k_cell_prep<<<p.num_sms * 8, kCellThreads, 0, s>>>(p);
+  return cudaGetLastError();
+}
+
+}  // namespace dbs

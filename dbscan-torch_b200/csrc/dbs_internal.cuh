@@ -1,0 +1,261 @@
+// dbs_internal.cuh -- shared types and device helpers of the sm_100a DBSCAN
+// pipeline. Not part of the public C-ABI (include/dbscan_b200.h).
+//
+// Pipeline (one stream, no host synchronisation; every count that sizes a
+// loop lives in device memory, so the whole sequence can be captured in a
+// CUDA graph):
+//
+//   k_init         zero per-call counters, histograms, per-cloud bounds
+//   k_bounds       per-cloud bounds of the cell coordinates (kx, ky)
+//   k_seg_finalize per-cloud compacted key ranges, key bases, pass count
+//   k_keys_hist    compacted cell keys + every radix digit's histogram
+//   k_onesweep x8  LSD radix passes with decoupled look-back; passes past the
+//                  device-side pass count return at once; the last real pass
+//                  also gathers the sorted float2 coordinates and perm
+//   k_rle          run-length cells: cell_start, cell_key, cell map
+//   k_cell_prep    per-cell bounding box + 25-entry neighbour table
+//   k_core         core flags (warp-cooperative counts) + cell status
+//   k_union        cell-graph union-find over core cells
+//   k_ids          flatten + exclusive scan of root flags (look-back)
+//   k_labels       core labels, border assignment, unpermute
+//
+// The plain call is the batched call with one cloud: every kernel works on
+// a segmented layout (clouds concatenated, each with its own eps and
+// min_samples, disjoint key ranges).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace dbs {
+
+constexpr int kRadixBits = 8;
+constexpr int kRadix = 1 << kRadixBits;
+constexpr int kMaxPasses = 64 / kRadixBits;
+constexpr int kSortThreads = 256;
+constexpr int kSortWarps = kSortThreads / 32;
+constexpr int kSortItems = 16;
+constexpr int kSortTile = kSortThreads * kSortItems;
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 16;
+constexpr int kScanTile = kScanThreads * kScanItems;
+constexpr int kCellThreads = 256;               // warp-per-cell kernels
+constexpr uint32_t kSpinCap = 1u << 22;         // bounded waits (look-back polls)
+constexpr uint32_t kFindCap = 1u << 20;         // bounded union-find walks / retries
+constexpr int kNgh = 25;
+
+// Dense cell map: a cloud whose compacted key range W satisfies
+// W <= kDenseFactor * N + kDenseSlack resolves neighbours with one load.
+constexpr int64_t kDenseFactor = 4;
+constexpr int64_t kDenseSlack = 4096;
+
+// Error bits of Desc::status (OR-ed by kernels, read by the host).
+enum : uint32_t {
+  kErrLookback = 1u << 0,   // a decoupled look-back wait hit its cap
+  kErrFind = 1u << 1,       // a union-find walk / hook loop hit its cap
+  kErrKeySpace = 1u << 2,   // batched key ranges overflow 64 bits
+};
+
+// Dynamic work counters (Desc::ctr).
+enum : int {
+  kCtrPass0 = 0,            // kMaxPasses counters, one per onesweep pass
+  kCtrRle = kMaxPasses,
+  kCtrPrep,
+  kCtrCore,
+  kCtrUnion,
+  kCtrIds,
+  kCtrLabels,
+  kCtrDebug,
+  kNumCtr
+};
+
+// Host-computed per-cloud scalars (dbscan_cuda.cu:547-550 of the reference:
+// fl_eps = (float)eps, inv_r = sqrtf(2)/fl_eps, eps_sq = fl_eps*fl_eps on
+// the host in IEEE float, ms = (int32)min_samples).
+struct SegParam {
+  float inv_r;
+  float eps_sq;
+  int32_t ms;
+  int32_t pad;
+};
+
+// Device-computed per-cloud layout. Cell coordinates are split into the
+// non-negative and negative classes so that the compaction preserves the
+// reference's unsigned key order ((u32)kx << 32 | (u32)ky): non-negative
+// coordinates come first, then negative ones, each class ascending.
+struct SegInfo {
+  int32_t bx[4];     // x: lo_pos, hi_pos, lo_neg, hi_neg (atomics)
+  int32_t by[4];     // y: same
+  uint64_t px, wx;   // x: width of the non-negative class, total width
+  uint64_t py, wy;   // y: same
+  uint64_t base;     // first global key of this cloud
+  int64_t map_base;  // offset in the dense cell map, -1 when not dense
+  int32_t cell_begin;  // first cell index of this cloud (filled by k_rle)
+  int32_t pad;
+};
+
+struct Desc {
+  uint32_t status;
+  uint32_t key64;      // keys stored as u64 (else u32)
+  uint32_t nbits;      // significant key bits
+  uint32_t npasses;    // radix passes that run (>= 1)
+  uint32_t num_cells;
+  uint32_t pad0;
+  uint64_t dense_total;  // dense-map entries in use
+  uint32_t ctr[kNumCtr];
+  uint32_t hist[kMaxPasses][kRadix];
+};
+
+// Device pointers of one call, carved out of the caller's workspace.
+struct Plan {
+  Desc* desc;
+  const float2* X;        // (n) input points, AoS
+  int32_t* labels;        // (n) output labels, input order
+  int64_t* seg_off;       // (nseg+1)
+  SegParam* seg_param;    // (nseg)
+  SegInfo* seg_info;
+  void* keys[2];          // ping-pong key buffers (u32 or u64 elements)
+  uint32_t* vals[2];      // ping-pong index buffers
+  uint32_t* perm;         // (n) sorted position -> input index
+  float2* xy;             // (n) sorted coordinates
+  uint8_t* is_core;       // (n) sorted order
+  unsigned long long* sweep_status[2];  // onesweep look-back words
+  unsigned long long* rle_status;
+  unsigned long long* ids_status;
+  int32_t* cell_start;    // (n+1)
+  uint64_t* cell_key;     // (n)
+  int32_t* cell_seg;      // (n)
+  float4* bbox;           // (n) xmin, xmax, ymin, ymax
+  int32_t* ngh;           // (n*25)
+  uint8_t* cell_status;   // (n) 0 none, 1 mixed, 2 all core
+  int32_t* uf;            // (n)
+  int32_t* root_rank;     // (n) exclusive scan of root flags
+  int32_t* cell_map;      // dense cell map
+  int64_t dense_cap;      // entries available in cell_map
+  int64_t n;
+  int32_t nseg;
+  int32_t sweep_tiles;    // ceil(n / kSortTile)
+  int32_t scan_tiles;     // ceil(n / kScanTile)
+  int32_t num_sms;
+  int32_t single;         // one cloud: k_init writes seg_off / seg_param
+  SegParam single_param;
+};
+
+// ------------------------------------------------------------- device math
+// Every operation below is IEEE round-to-nearest with subnormals flushed
+// (the library is compiled with -ftz=true -fmad=false), matching the
+// reference build's --use_fast_math arithmetic on the values it produces.
+__device__ __forceinline__ float sq_dist(float ex, float ey) {
+  // fma(ex, ex, ey*ey): the contraction of `ex*ex + ey*ey` found in the
+  // reference build at every call site.
+  return __fmaf_rn(ex, ex, __fmul_rn(ey, ey));
+}
+
+// dbscan_cuda.cu:183-187
+__device__ __forceinline__ float point_box_d2(float x, float y, float4 b) {
+  float dx = fmaxf(fmaxf(__fsub_rn(b.x, x), __fsub_rn(x, b.y)), 0.0f);
+  float dy = fmaxf(fmaxf(__fsub_rn(b.z, y), __fsub_rn(y, b.w)), 0.0f);
+  return sq_dist(dx, dy);
+}
+
+// dbscan_cuda.cu:190-194
+__device__ __forceinline__ float box_box_d2(float4 a, float4 b) {
+  float dx = fmaxf(fmaxf(__fsub_rn(b.x, a.y), __fsub_rn(a.x, b.y)), 0.0f);
+  float dy = fmaxf(fmaxf(__fsub_rn(b.z, a.w), __fsub_rn(a.z, b.w)), 0.0f);
+  return sq_dist(dx, dy);
+}
+
+// (int32)floorf(v): round toward -inf, saturating, NaN -> 0.
+__device__ __forceinline__ int32_t cell_coord(float v, float inv_r) {
+  return __float2int_rd(__fmul_rn(v, inv_r));
+}
+
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+  uint32_t m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+// Segment (cloud) of input/sorted position i. Points of a cloud are
+// contiguous in input order and, because cloud key ranges are disjoint and
+// ascending, in sorted order too.
+__device__ __forceinline__ int32_t seg_of(const Plan& p, int64_t i) {
+  if (p.nseg == 1) return 0;
+  int32_t lo = 0, hi = p.nseg - 1;
+  while (lo < hi) {
+    int32_t mid = (lo + hi + 1) >> 1;
+    if (p.seg_off[mid] <= i) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Compacted coordinate of kx along one axis, or -1 (as u64 ~0) when the
+// coordinate is outside the cloud's occupied classes.
+__device__ __forceinline__ uint64_t compact_axis(int32_t k, const int32_t b[4], uint64_t pw) {
+  if (k >= 0) {
+    if (b[1] < 0 || k < b[0] || k > b[1]) return ~0ull;
+    return (uint64_t)(uint32_t)(k - b[0]);
+  }
+  if (b[2] == 0 || k < b[2] || k > b[3]) return ~0ull;
+  return pw + (uint64_t)(uint32_t)(k - b[2]);
+}
+
+__device__ __forceinline__ int32_t expand_axis(uint64_t g, const int32_t b[4], uint64_t pw) {
+  if (g < pw) return (int32_t)((uint32_t)b[0] + (uint32_t)g);
+  return (int32_t)((uint32_t)b[2] + (uint32_t)(g - pw));
+}
+
+__device__ __forceinline__ void set_error(Desc* d, uint32_t bits) {
+  atomicOr(&d->status, bits);
+}
+
+// Relaxed device-scope 64-bit load/store for look-back words.
+__device__ __forceinline__ unsigned long long ld_relaxed(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_relaxed(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" :: "l"(p), "l"(v) : "memory");
+}
+
+constexpr unsigned long long kFlagAgg = 1ull << 62;
+constexpr unsigned long long kFlagInc = 2ull << 62;
+constexpr unsigned long long kValMask = (1ull << 62) - 1;
+
+// Decoupled look-back over look-back words laid out with `stride` between
+// consecutive tiles. Returns the exclusive prefix of tile `tile`. Bounded:
+// a wait that exceeds kSpinCap polls sets kErrLookback and gives up.
+__device__ __forceinline__ unsigned long long lookback(const unsigned long long* words,
+                                                       int64_t tile, int64_t stride, Desc* d) {
+  unsigned long long excl = 0;
+  int64_t j = tile - 1;
+  uint32_t spins = 0;
+  while (j >= 0) {
+    unsigned long long v = ld_relaxed(words + j * stride);
+    unsigned long long flag = v & ~kValMask;
+    if (flag == 0) {
+      if (++spins > kSpinCap) { set_error(d, kErrLookback); break; }
+      continue;
+    }
+    excl += v & kValMask;
+    if (flag == kFlagInc) break;
+    --j;
+  }
+  return excl;
+}
+
+// --------------------------------------------------------- host launchers
+// Each returns cudaGetLastError() of its launches.
+cudaError_t launch_front(const Plan& p, cudaStream_t s);      // init, bounds, finalize, keys_hist
+cudaError_t launch_sort_pass(const Plan& p, int pass, cudaStream_t s);
+cudaError_t launch_rle(const Plan& p, cudaStream_t s);
+cudaError_t launch_cell_prep(const Plan& p, cudaStream_t s);
+cudaError_t launch_core(const Plan& p, cudaStream_t s);
+cudaError_t launch_union(const Plan& p, cudaStream_t s);
+cudaError_t launch_ids(const Plan& p, cudaStream_t s);
+cudaError_t launch_labels(const Plan& p, cudaStream_t s);
+
+}  // namespace dbs

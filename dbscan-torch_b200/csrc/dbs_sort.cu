@@ -1,0 +1,490 @@
+// dbs_sort.cu -- grid hashing and the LSD onesweep radix sort.
+//
+// Reference path replaced (ryanirl/dbscan-torch v0.2.0, csrc/cuda/dbscan_cuda.cu):
+//   k_cell_keys :55-66, thrust::sort_by_key :582-586, k_gather_xy :71-79.
+//
+// Keys. The reference sorts u64 keys (u32)kx << 32 | (u32)ky. Here each cloud
+// first reduces the bounds of its cell coordinates, split into the
+// non-negative and the negative class per axis; the compacted coordinate
+// (non-negative class first, then the negative class, each ascending) is a
+// strictly increasing function of the u32 coordinate, so
+//   key = base[cloud] + gx * wy + gy
+// sorts exactly like the reference key while needing only
+// ceil(log2(sum of ranges)) bits: 22 bits (three 8-bit passes) for a
+// 10M-point constant-density cloud instead of eight passes. Keys are stored
+// as u32 when they fit, else u64 (decided on the device).
+//
+// Sort. One histogram pass computes every digit's 256-bin histogram; each
+// onesweep pass then ranks a 4096-key tile in shared memory (warp match
+// ranking, stable), resolves its global digit offsets by decoupled look-back
+// over per-(tile, digit) words, and scatters through a shared-memory staging
+// buffer so each digit run is written contiguously. Tiles are taken in
+// launch order from an atomic counter, so a tile only waits on tiles whose
+// blocks are already running. The last pass writes perm and gathers the
+// float2 coordinates (the reference's k_gather_xy) in the same scatter.
+#include "dbs_internal.cuh"
+
+namespace dbs {
+
+// ----------------------------------------------------------------- k_init
+__global__ void k_init(Plan p) {
+  const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  Desc* d = p.desc;
+  if (tid == 0) {
+    d->status = 0;
+    d->key64 = 0;
+    d->nbits = 0;
+    d->npasses = 1;
+    d->num_cells = 0;
+    d->dense_total = 0;
+  }
+  if (p.single && tid == 0) {
+    p.seg_off[0] = 0;
+    p.seg_off[1] = p.n;
+    p.seg_param[0] = p.single_param;
+  }
+  for (int64_t i = tid; i < kNumCtr; i += stride) d->ctr[i] = 0;
+  for (int64_t i = tid; i < kMaxPasses * kRadix; i += stride) (&d->hist[0][0])[i] = 0;
+  for (int64_t s = tid; s < p.nseg; s += stride) {
+    SegInfo& g = p.seg_info[s];
+    g.bx[0] = INT32_MAX; g.bx[1] = -1; g.bx[2] = 0; g.bx[3] = INT32_MIN;
+    g.by[0] = INT32_MAX; g.by[1] = -1; g.by[2] = 0; g.by[3] = INT32_MIN;
+    g.cell_begin = 0;
+  }
+}
+
+// --------------------------------------------------------------- k_bounds
+// Per-cloud class bounds. Each thread folds a run of points of one cloud and
+// flushes with atomics when the cloud changes.
+struct AxisAcc {
+  int32_t lo_pos, hi_pos, lo_neg, hi_neg;
+  __device__ void reset() { lo_pos = INT32_MAX; hi_pos = -1; lo_neg = 0; hi_neg = INT32_MIN; }
+  __device__ void add(int32_t k) {
+    if (k >= 0) { lo_pos = min(lo_pos, k); hi_pos = max(hi_pos, k); }
+    else { lo_neg = min(lo_neg, k); hi_neg = max(hi_neg, k); }
+  }
+  __device__ void flush(int32_t* b) {
+    if (hi_pos >= 0) { atomicMin(&b[0], lo_pos); atomicMax(&b[1], hi_pos); }
+    if (lo_neg < 0) { atomicMin(&b[2], lo_neg); atomicMax(&b[3], hi_neg); }
+  }
+};
+
+__device__ __forceinline__ void warp_fold(AxisAcc& a) {
+  const uint32_t full = 0xffffffffu;
+  a.lo_pos = __reduce_min_sync(full, a.lo_pos);
+  a.hi_pos = __reduce_max_sync(full, a.hi_pos);
+  a.lo_neg = __reduce_min_sync(full, a.lo_neg);
+  a.hi_neg = __reduce_max_sync(full, a.hi_neg);
+}
+
+__global__ void __launch_bounds__(256) k_bounds(Plan p) {
+  const int64_t n = p.n;
+  // Each block owns a contiguous chunk; within it, lanes read consecutive
+  // points (coalesced float2 loads).
+  const int64_t per_block = (n + gridDim.x - 1) / gridDim.x;
+  const int64_t b0 = (int64_t)blockIdx.x * per_block;
+  const int64_t b1 = min(n, b0 + per_block);
+  if (b0 >= b1) return;
+  int32_t seg = seg_of(p, b0);
+  int64_t seg_end = p.seg_off[seg + 1];
+  float inv_r = p.seg_param[seg].inv_r;
+  AxisAcc ax, ay;
+  ax.reset(); ay.reset();
+  for (int64_t base = b0; base < b1; base += blockDim.x) {
+    const int64_t i = base + threadIdx.x;
+    // The cloud of the whole block-row: when the row is inside one cloud
+    // (the common case) the warp folds its partial bounds before flushing.
+    while (base >= seg_end) {
+      // block-uniform advance to the cloud containing `base`
+      ++seg;
+      seg_end = p.seg_off[seg + 1];
+      inv_r = p.seg_param[seg].inv_r;
+    }
+    const bool row_in_seg = (min(base + (int64_t)blockDim.x, b1) <= seg_end);
+    if (row_in_seg) {
+      if (i < b1) {
+        float2 v = p.X[i];
+        ax.add(cell_coord(v.x, inv_r));
+        ay.add(cell_coord(v.y, inv_r));
+      }
+    } else {
+      // Row straddles clouds: fold the running accumulators first, then
+      // handle each point with its own cloud's atomics.
+      warp_fold(ax); warp_fold(ay);
+      if (lane_id() == 0) { ax.flush(p.seg_info[seg].bx); ay.flush(p.seg_info[seg].by); }
+      ax.reset(); ay.reset();
+      if (i < b1) {
+        const int32_t s = seg_of(p, i);
+        const float ir = p.seg_param[s].inv_r;
+        float2 v = p.X[i];
+        AxisAcc tx, ty;
+        tx.reset(); ty.reset();
+        tx.add(cell_coord(v.x, ir));
+        ty.add(cell_coord(v.y, ir));
+        tx.flush(p.seg_info[s].bx);
+        ty.flush(p.seg_info[s].by);
+      }
+      // Continue with the cloud of the last point of this row.
+      const int64_t last = min(base + (int64_t)blockDim.x, b1) - 1;
+      while (last >= seg_end) {
+        ++seg;
+        seg_end = p.seg_off[seg + 1];
+        inv_r = p.seg_param[seg].inv_r;
+      }
+    }
+    // Flush when the next row starts in another cloud.
+    const int64_t next = base + blockDim.x;
+    if (next < b1 && next >= seg_end) {
+      warp_fold(ax); warp_fold(ay);
+      if (lane_id() == 0) { ax.flush(p.seg_info[seg].bx); ay.flush(p.seg_info[seg].by); }
+      ax.reset(); ay.reset();
+    }
+  }
+  warp_fold(ax); warp_fold(ay);
+  if (lane_id() == 0) { ax.flush(p.seg_info[seg].bx); ay.flush(p.seg_info[seg].by); }
+}
+
+// --------------------------------------------------------- k_seg_finalize
+// One block: per-cloud class widths, key bases (exclusive scan of the
+// per-cloud ranges), dense-map bases, and the global key width.
+__global__ void __launch_bounds__(1024) k_seg_finalize(Plan p) {
+  __shared__ unsigned long long s_range[1024];
+  __shared__ unsigned long long s_dense[1024];
+  __shared__ unsigned long long s_carry_range, s_carry_dense;
+  __shared__ int s_overflow;
+  if (threadIdx.x == 0) { s_carry_range = 0; s_carry_dense = 0; s_overflow = 0; }
+  __syncthreads();
+  for (int32_t s0 = 0; s0 < p.nseg; s0 += blockDim.x) {
+    const int32_t s = s0 + threadIdx.x;
+    unsigned long long range = 0, dense = 0;
+    bool sat = false;
+    if (s < p.nseg) {
+      SegInfo& g = p.seg_info[s];
+      const uint64_t npx = g.bx[1] >= 0 ? (uint64_t)((int64_t)g.bx[1] - g.bx[0] + 1) : 0;
+      const uint64_t nnx = g.bx[2] < 0 ? (uint64_t)((int64_t)g.bx[3] - g.bx[2] + 1) : 0;
+      const uint64_t npy = g.by[1] >= 0 ? (uint64_t)((int64_t)g.by[1] - g.by[0] + 1) : 0;
+      const uint64_t nny = g.by[2] < 0 ? (uint64_t)((int64_t)g.by[3] - g.by[2] + 1) : 0;
+      g.px = npx; g.wx = npx + nnx;
+      g.py = npy; g.wy = npy + nny;
+      const int64_t npts = p.seg_off[s + 1] - p.seg_off[s];
+      if (npts > 0) {
+        // range = wx * wy, saturating (only one full-range cloud fits 64 bits)
+        if (g.wx != 0 && g.wy > (~0ull) / g.wx) { sat = true; range = ~0ull; }
+        else range = g.wx * g.wy;
+        const unsigned long long cap = (unsigned long long)(kDenseFactor * npts + kDenseSlack);
+        if (!sat && range <= cap) dense = range;
+      }
+    }
+    s_range[threadIdx.x] = range;
+    s_dense[threadIdx.x] = dense;
+    if (sat && p.nseg > 1) atomicOr(&s_overflow, 1);
+    __syncthreads();
+    // Inclusive Hillis-Steele scan (saturating for ranges).
+    for (int off = 1; off < (int)blockDim.x; off <<= 1) {
+      unsigned long long r = 0, dn = 0;
+      if ((int)threadIdx.x >= off) { r = s_range[threadIdx.x - off]; dn = s_dense[threadIdx.x - off]; }
+      __syncthreads();
+      if ((int)threadIdx.x >= off) {
+        unsigned long long a = s_range[threadIdx.x];
+        unsigned long long sum = a + r;
+        if (sum < a) { sum = ~0ull; atomicOr(&s_overflow, 1); }
+        s_range[threadIdx.x] = sum;
+        s_dense[threadIdx.x] += dn;
+      }
+      __syncthreads();
+    }
+    if (s < p.nseg) {
+      SegInfo& g = p.seg_info[s];
+      const unsigned long long incl = s_range[threadIdx.x];
+      unsigned long long base = s_carry_range + (incl - range);
+      if (base < s_carry_range) atomicOr(&s_overflow, 1);
+      g.base = base;
+      g.map_base = dense > 0 ? (int64_t)(s_carry_dense + s_dense[threadIdx.x] - dense) : -1;
+    }
+    __syncthreads();
+    if (threadIdx.x == blockDim.x - 1) {
+      unsigned long long t = s_carry_range + s_range[threadIdx.x];
+      if (t < s_carry_range) s_overflow = 1;
+      s_carry_range = t;
+      s_carry_dense += s_dense[threadIdx.x];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    Desc* d = p.desc;
+    // The last key is base[last] + range[last] - 1 (fits even when the sum
+    // of ranges is exactly 2^64 for a single cloud).
+    unsigned long long max_key = s_carry_range == 0 ? 0 : s_carry_range - 1;
+    if (p.nseg == 1) {
+      const SegInfo& g = p.seg_info[0];
+      max_key = (g.wx == 0 || g.wy == 0) ? 0 : (g.wx - 1) * g.wy + (g.wy - 1);
+    }
+    uint32_t nbits = max_key == 0 ? 0 : 64 - __clzll((long long)max_key);
+    uint32_t np = (nbits + kRadixBits - 1) / kRadixBits;
+    d->nbits = nbits;
+    d->npasses = np < 1 ? 1 : np;
+    d->key64 = nbits > 32 ? 1 : 0;
+    unsigned long long dt = s_carry_dense;
+    if ((long long)dt > p.dense_cap) dt = 0;  // cannot happen by construction
+    d->dense_total = dt;
+    if (s_overflow) set_error(d, kErrKeySpace);
+  }
+}
+
+// ------------------------------------------------------------ k_keys_hist
+template <typename K>
+__device__ __forceinline__ void keys_hist_body(const Plan& p, uint32_t (*sh)[kRadix], uint32_t npasses) {
+  const int64_t n = p.n;
+  K* keys = reinterpret_cast<K*>(p.keys[0]);
+  const int64_t per_block = (n + gridDim.x - 1) / gridDim.x;
+  const int64_t b0 = (int64_t)blockIdx.x * per_block;
+  const int64_t b1 = min(n, b0 + per_block);
+  int32_t seg = b0 < b1 ? seg_of(p, b0) : 0;
+  for (int64_t i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
+    while (i >= p.seg_off[seg + 1]) ++seg;
+    const SegInfo& g = p.seg_info[seg];
+    const float inv_r = p.seg_param[seg].inv_r;
+    const float2 v = p.X[i];
+    const uint64_t gx = compact_axis(cell_coord(v.x, inv_r), g.bx, g.px);
+    const uint64_t gy = compact_axis(cell_coord(v.y, inv_r), g.by, g.py);
+    const uint64_t key = g.base + gx * g.wy + gy;
+    keys[i] = (K)key;
+    for (uint32_t ps = 0; ps < npasses; ++ps)
+      atomicAdd(&sh[ps][(key >> (ps * kRadixBits)) & (kRadix - 1)], 1u);
+  }
+}
+
+__global__ void __launch_bounds__(256) k_keys_hist(Plan p) {
+  __shared__ uint32_t sh[kMaxPasses][kRadix];
+  Desc* d = p.desc;
+  const uint32_t npasses = d->npasses;
+  for (int i = threadIdx.x; i < kMaxPasses * kRadix; i += blockDim.x) (&sh[0][0])[i] = 0;
+  __syncthreads();
+  if (d->key64) keys_hist_body<uint64_t>(p, sh, npasses);
+  else keys_hist_body<uint32_t>(p, sh, npasses);
+  __syncthreads();
+  for (int i = threadIdx.x; i < (int)npasses * kRadix; i += blockDim.x) {
+    const uint32_t v = (&sh[0][0])[i];
+    if (v) atomicAdd(&(&d->hist[0][0])[i], v);
+  }
+  // Clearing duties for later kernels (their look-back words and the dense
+  // cell map must start empty).
+  const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t nsweep = (int64_t)p.sweep_tiles * kRadix;
+  for (int64_t i = tid; i < nsweep; i += stride) p.sweep_status[0][i] = 0;
+  for (int64_t i = tid; i < p.scan_tiles; i += stride) { p.rle_status[i] = 0; p.ids_status[i] = 0; }
+  const int64_t dense = (int64_t)d->dense_total;
+  for (int64_t i = tid; i < dense; i += stride) p.cell_map[i] = -1;
+}
+
+// ------------------------------------------------------------- k_onesweep
+struct SweepSmem {
+  uint32_t wcnt[kSortWarps][kRadix];   // per-warp digit counts -> warp offsets
+  uint32_t tile_excl[kRadix];          // exclusive scan of tile digit counts
+  uint32_t glob[kRadix];               // global position of each digit run
+  uint32_t bucket[kRadix];             // exclusive scan of the digit histogram
+  uint32_t warp_tot[kSortWarps];
+  uint32_t tile;
+};
+
+template <typename K>
+__device__ __forceinline__ void onesweep_body(const Plan& p, int pass, bool last, SweepSmem& sm,
+                                              unsigned char* stage_raw) {
+  const int64_t n = p.n;
+  const uint32_t lane = lane_id();
+  const uint32_t warp = threadIdx.x >> 5;
+  const uint32_t shift = pass * kRadixBits;
+  const int src = pass & 1;
+  const K* keys_in = reinterpret_cast<const K*>(p.keys[src]);
+  K* keys_out = reinterpret_cast<K*>(p.keys[src ^ 1]);
+  const uint32_t* vals_in = p.vals[src];
+  uint32_t* vals_out = last ? p.perm : p.vals[src ^ 1];
+  K* st_keys = reinterpret_cast<K*>(stage_raw);
+  uint32_t* st_vals = reinterpret_cast<uint32_t*>(stage_raw + sizeof(K) * kSortTile);
+  unsigned long long* words = p.sweep_status[pass & 1];
+  Desc* d = p.desc;
+
+  // Bucket bases: exclusive scan of this digit's global histogram.
+  {
+    const uint32_t t = threadIdx.x;
+    uint32_t v = d->hist[pass][t];
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= (uint32_t)o) x += y;
+    }
+    if (lane == 31) sm.warp_tot[warp] = x;
+    __syncthreads();
+    uint32_t wpre = 0;
+    for (uint32_t w = 0; w < warp; ++w) wpre += sm.warp_tot[w];
+    sm.bucket[t] = wpre + x - v;
+    __syncthreads();
+  }
+
+  // Clear the other look-back region for the next pass.
+  {
+    unsigned long long* other = p.sweep_status[(pass & 1) ^ 1];
+    const int64_t total = (int64_t)p.sweep_tiles * kRadix;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+         i += (int64_t)gridDim.x * blockDim.x)
+      other[i] = 0;
+  }
+
+  while (true) {
+    if (threadIdx.x == 0) sm.tile = atomicAdd(&d->ctr[kCtrPass0 + pass], 1u);
+    for (int i = threadIdx.x; i < kSortWarps * kRadix; i += blockDim.x) (&sm.wcnt[0][0])[i] = 0;
+    __syncthreads();
+    const uint32_t tile = sm.tile;
+    if ((int64_t)tile >= p.sweep_tiles) break;
+    const int64_t tile_base = (int64_t)tile * kSortTile;
+    const int64_t wbase = tile_base + (int64_t)warp * 32 * kSortItems;
+
+    K key[kSortItems];
+    uint32_t val[kSortItems];
+    uint32_t dig[kSortItems];
+    uint32_t rank[kSortItems];
+#pragma unroll
+    for (int k = 0; k < kSortItems; ++k) {
+      const int64_t gi = wbase + k * 32 + lane;
+      if (gi < n) {
+        key[k] = keys_in[gi];
+        val[k] = pass == 0 ? (uint32_t)gi : vals_in[gi];
+        dig[k] = (uint32_t)((uint64_t)key[k] >> shift) & (kRadix - 1);
+      } else {
+        key[k] = 0; val[k] = 0; dig[k] = kRadix;  // sentinel digit
+      }
+    }
+    // Stable warp ranking: items in (k, lane) order.
+#pragma unroll
+    for (int k = 0; k < kSortItems; ++k) {
+      const uint32_t dk = dig[k];
+      const uint32_t peers = __match_any_sync(0xffffffffu, dk);
+      const uint32_t leader = __ffs(peers) - 1;
+      uint32_t old = 0;
+      if (lane == leader && dk < kRadix) {
+        old = sm.wcnt[warp][dk];
+        sm.wcnt[warp][dk] = old + __popc(peers);
+      }
+      old = __shfl_sync(0xffffffffu, old, leader);
+      rank[k] = old + __popc(peers & lanemask_lt());
+      __syncwarp();
+    }
+    __syncthreads();
+    // Per digit: warp exclusive offsets and the tile count.
+    uint32_t tile_cnt;
+    {
+      const uint32_t t = threadIdx.x;
+      uint32_t run = 0;
+#pragma unroll
+      for (int w = 0; w < kSortWarps; ++w) {
+        const uint32_t c = sm.wcnt[w][t];
+        sm.wcnt[w][t] = run;
+        run += c;
+      }
+      tile_cnt = run;
+      // Publish this tile's aggregate (or inclusive prefix for tile 0).
+      unsigned long long* my = words + (int64_t)tile * kRadix + t;
+      if (tile == 0) st_relaxed(my, kFlagInc | (unsigned long long)tile_cnt);
+      else st_relaxed(my, kFlagAgg | (unsigned long long)tile_cnt);
+      // Block exclusive scan of tile counts over digits.
+      uint32_t x = tile_cnt;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= (uint32_t)o) x += y;
+      }
+      if (lane == 31) sm.warp_tot[warp] = x;
+      __syncthreads();
+      uint32_t wpre = 0;
+      for (uint32_t w = 0; w < warp; ++w) wpre += sm.warp_tot[w];
+      sm.tile_excl[t] = wpre + x - tile_cnt;
+      // Look-back for digit t.
+      unsigned long long excl = 0;
+      if (tile > 0) {
+        excl = lookback(words + t, tile, kRadix, d);
+        st_relaxed(my, kFlagInc | (excl + tile_cnt));
+      }
+      sm.glob[t] = sm.bucket[t] + (uint32_t)excl;
+    }
+    __syncthreads();
+    // Stage into shared memory in tile-sorted order.
+#pragma unroll
+    for (int k = 0; k < kSortItems; ++k) {
+      const uint32_t dk = dig[k];
+      if (dk < kRadix) {
+        const uint32_t lp = sm.tile_excl[dk] + sm.wcnt[warp][dk] + rank[k];
+        st_keys[lp] = key[k];
+        st_vals[lp] = val[k];
+      }
+    }
+    __syncthreads();
+    const int32_t valid = (int32_t)min((int64_t)kSortTile, n - tile_base);
+    for (int32_t lp = threadIdx.x; lp < valid; lp += blockDim.x) {
+      const K kk = st_keys[lp];
+      const uint32_t dk = (uint32_t)((uint64_t)kk >> shift) & (kRadix - 1);
+      const uint32_t gpos = sm.glob[dk] + (uint32_t)lp - sm.tile_excl[dk];
+      const uint32_t vv = st_vals[lp];
+      if ((int64_t)gpos >= n) continue;  // only after a failed look-back
+      keys_out[gpos] = kk;
+      vals_out[gpos] = vv;
+      if (last) p.xy[gpos] = p.X[vv];
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(kSortThreads) k_onesweep(Plan p, int pass) {
+  extern __shared__ __align__(16) unsigned char dyn_smem[];
+  SweepSmem& sm = *reinterpret_cast<SweepSmem*>(dyn_smem);
+  unsigned char* stage = dyn_smem + ((sizeof(SweepSmem) + 15) & ~size_t(15));
+  const Desc* d = p.desc;
+  const int np = (int)d->npasses;
+  if (pass >= np) return;
+  const bool last = pass == np - 1;
+  if (d->key64) onesweep_body<uint64_t>(p, pass, last, sm, stage);
+  else onesweep_body<uint32_t>(p, pass, last, sm, stage);
+}
+
+constexpr size_t kSweepSmemBytes =
+    ((sizeof(SweepSmem) + 15) & ~size_t(15)) + (sizeof(uint64_t) + sizeof(uint32_t)) * kSortTile;
+
+// ------------------------------------------------------------- launchers
+static int grid_for(const Plan& p, int64_t work, int threads, int per_sm) {
+  int64_t g = (work + threads - 1) / threads;
+  const int64_t cap = (int64_t)p.num_sms * per_sm;
+  if (g > cap) g = cap;
+  if (g < 1) g = 1;
+  return (int)g;
+}
+
+cudaError_t launch_front(const Plan& p, cudaStream_t s) {
+  k_init<<<grid_for(p, kMaxPasses * kRadix, 256, 1), 256, 0, s>>>(p);
+  k_bounds<<<grid_for(p, p.n, 256 * 8, 8), 256, 0, s>>>(p);
+  k_seg_finalize<<<1, 1024, 0, s>>>(p);
+  k_keys_hist<<<grid_for(p, p.n, 256 * 8, 8), 256, 0, s>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sort_pass(const Plan& p, int pass, cudaStream_t s) {
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaError_t e = cudaFuncSetAttribute(k_onesweep, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kSweepSmemBytes);
+    if (e != cudaSuccess) return e;
+    attr_set = true;
+  }
+  // Persistent grid: blocks loop over tiles taken from an atomic counter.
+  int blocks_per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_onesweep, kSortThreads,
+                                                kSweepSmemBytes);
+  if (blocks_per_sm < 1) blocks_per_sm = 1;
+  int grid = p.num_sms * blocks_per_sm;
+  if (grid > p.sweep_tiles) grid = p.sweep_tiles > 0 ? p.sweep_tiles : 1;
+  k_onesweep<<<grid, kSortThreads, kSweepSmemBytes, s>>>(p, pass);
+  return cudaGetLastError();
+}
+
+}  // namespace dbs

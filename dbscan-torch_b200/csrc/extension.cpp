@@ -1,0 +1,390 @@
+// extension.cpp -- the pybind module `dbscan_torch._C`.
+//
+// Same entry points, argument names, validation order and error strings as
+// the reference's csrc/extension.cpp (ryanirl/dbscan-torch v0.2.0):
+//   check_input          extension.cpp:26-31
+//   dbscan2d             extension.cpp:33-45, 67-70
+//   dbscan2d_profile     extension.cpp:52-63, 71-74
+//   dbscan2d_cuda_debug  extension.cpp:76-79 (layout dbscan_cuda.cu:777-789)
+// plus the batched form. Every call goes through the C-ABI of
+// include/dbscan_b200.h (libdbscan_b200.so); there is no CPU implementation:
+// a CPU tensor is copied to the current CUDA device, clustered there and the
+// labels copied back (the reference ran its CPU path for CPU tensors; this
+// build has only the GPU path and says so when no GPU is present).
+//
+// Device-side failures (a bounded wait that ran out) are recorded in the
+// call's workspace. The call does not synchronise; the status word is copied
+// asynchronously into a pinned slot and checked at the next call on that
+// thread or by check_status(), which raises RuntimeError.
+#include <ATen/cuda/CUDAContext.h>
+#include <c10/cuda/CUDAGuard.h>
+#include <torch/extension.h>
+
+#include <cstdlib>
+#include <map>
+#include <mutex>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../../include/dbscan_b200.h"
+
+namespace {
+
+void check_input(const torch::Tensor& X, double eps, int64_t min_samples) {
+  TORCH_CHECK(X.dim() == 2 && X.size(1) == 2, "X must have shape (N, 2)");
+  TORCH_CHECK(X.scalar_type() == torch::kFloat32, "X must be float32");
+  TORCH_CHECK(eps > 0.0, "eps must be > 0");
+  TORCH_CHECK(min_samples >= 1, "min_samples must be >= 1");
+}
+
+void check_rc(int rc, const char* what) {
+  TORCH_CHECK(rc == DBS_OK, what, ": ", dbs_strerror(rc), " (code ", rc, ")");
+}
+
+// ---------------------------------------------------------- status checks
+struct PendingStatus {
+  cudaEvent_t ev = nullptr;
+  uint32_t* host = nullptr;  // pinned
+  torch::Tensor ws;          // keeps the workspace alive until read
+  bool busy = false;
+};
+
+std::mutex g_mu;
+std::vector<PendingStatus> g_slots;
+size_t g_next = 0;
+constexpr size_t kSlots = 64;
+
+void raise_if_failed(uint32_t st) {
+  TORCH_CHECK(st == 0, "dbscan2d: device-side failure in an earlier call (status 0x",
+              std::hex, st, std::dec,
+              "): a bounded wait in the pipeline ran out; labels of that call are invalid");
+}
+
+// Checks completed slots (all slots, waiting, when `wait`).
+void drain(bool wait) {
+  std::lock_guard<std::mutex> lock(g_mu);
+  for (auto& s : g_slots) {
+    if (!s.busy) continue;
+    cudaError_t q = wait ? cudaEventSynchronize(s.ev) : cudaEventQuery(s.ev);
+    if (q == cudaErrorNotReady) continue;
+    C10_CUDA_CHECK(q);
+    s.busy = false;
+    s.ws = torch::Tensor();
+    const uint32_t st = *s.host;
+    raise_if_failed(st);
+  }
+}
+
+void enqueue_status(const torch::Tensor& ws, cudaStream_t stream) {
+  std::lock_guard<std::mutex> lock(g_mu);
+  if (g_slots.empty()) g_slots.resize(kSlots);
+  PendingStatus* slot = nullptr;
+  for (size_t k = 0; k < kSlots; ++k) {
+    PendingStatus& s = g_slots[(g_next + k) % kSlots];
+    if (!s.busy) { slot = &s; g_next = (g_next + k + 1) % kSlots; break; }
+  }
+  if (slot == nullptr) {
+    // All slots in flight: wait for the oldest.
+    PendingStatus& s = g_slots[g_next];
+    C10_CUDA_CHECK(cudaEventSynchronize(s.ev));
+    s.busy = false;
+    s.ws = torch::Tensor();
+    raise_if_failed(*s.host);
+    slot = &s;
+    g_next = (g_next + 1) % kSlots;
+  }
+  if (slot->ev == nullptr) {
+    C10_CUDA_CHECK(cudaEventCreateWithFlags(&slot->ev, cudaEventDisableTiming));
+    C10_CUDA_CHECK(cudaHostAlloc(reinterpret_cast<void**>(&slot->host), sizeof(uint32_t),
+                                 cudaHostAllocDefault));
+  }
+  *slot->host = 0;
+  // The status word is the first field of the workspace.
+  C10_CUDA_CHECK(cudaMemcpyAsync(slot->host, ws.data_ptr(), sizeof(uint32_t),
+                                 cudaMemcpyDeviceToHost, stream));
+  C10_CUDA_CHECK(cudaEventRecord(slot->ev, stream));
+  slot->ws = ws;
+  slot->busy = true;
+}
+
+bool sync_mode() {
+  static const bool on = [] {
+    const char* v = std::getenv("DBSCAN_TORCH_SYNC");
+    return v != nullptr && v[0] != '\0' && v[0] != '0';
+  }();
+  return on;
+}
+
+bool capturing(cudaStream_t s) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  C10_CUDA_CHECK(cudaStreamIsCapturing(s, &cs));
+  return cs != cudaStreamCaptureStatusNone;
+}
+
+torch::Tensor alloc_ws(size_t bytes, const torch::Device& dev) {
+  // The caching allocator returns 512-byte aligned blocks.
+  return torch::empty({(int64_t)bytes}, torch::TensorOptions().dtype(torch::kUInt8).device(dev));
+}
+
+void after_launch(const torch::Tensor& ws, cudaStream_t stream) {
+  if (capturing(stream)) return;
+  if (sync_mode()) {
+    uint32_t st = 0;
+    check_rc(dbs_read_status(ws.data_ptr(), stream, &st), "dbscan2d");
+    raise_if_failed(st);
+    return;
+  }
+  enqueue_status(ws, stream);
+}
+
+torch::Tensor require_cuda_copy(const torch::Tensor& X) {
+  TORCH_CHECK(torch::cuda::is_available(),
+              "dbscan_torch (B200 build) runs on a CUDA device only and none is available; "
+              "there is no CPU implementation in this build");
+  return X.to(torch::Device(torch::kCUDA, c10::cuda::current_device()),
+              /*non_blocking=*/X.is_pinned());
+}
+
+// Runs the plain pipeline on a contiguous CUDA tensor.
+torch::Tensor run_cuda(const torch::Tensor& Xc, double eps, int64_t min_samples) {
+  c10::cuda::CUDAGuard guard(Xc.device());
+  const int64_t n = Xc.size(0);
+  auto labels = torch::empty({n}, torch::TensorOptions().dtype(torch::kInt32).device(Xc.device()));
+  if (n == 0) return labels;
+  if (!capturing(at::cuda::getCurrentCUDAStream())) drain(false);
+  const size_t bytes = dbs_workspace_bytes(n, 1);
+  auto ws = alloc_ws(bytes, Xc.device());
+  cudaStream_t stream = at::cuda::getCurrentCUDAStream();
+  check_rc(dbs_dbscan2d(Xc.data_ptr<float>(), n, eps, min_samples, labels.data_ptr<int32_t>(),
+                        ws.data_ptr(), bytes, stream),
+           "dbscan2d");
+  after_launch(ws, stream);
+  return labels;
+}
+
+}  // namespace
+
+torch::Tensor dbscan2d(torch::Tensor X, double eps, int64_t min_samples) {
+  check_input(X, eps, min_samples);
+  if (X.is_cuda()) return run_cuda(X.contiguous(), eps, min_samples);
+  if (X.size(0) == 0)
+    return torch::empty({0}, torch::TensorOptions().dtype(torch::kInt32));
+  auto Xd = require_cuda_copy(X.contiguous());
+  auto labels = run_cuda(Xd, eps, min_samples);
+  return labels.to(torch::kCPU);
+}
+
+std::pair<torch::Tensor, std::map<std::string, float>> dbscan2d_profile(torch::Tensor X, double eps,
+                                                                        int64_t min_samples) {
+  check_input(X, eps, min_samples);
+  const bool host = !X.is_cuda();
+  torch::Tensor Xc = X.contiguous();
+  std::map<std::string, float> out;
+  for (int i = 0; i < DBS_NUM_STAGES; ++i) out[dbs_stage_name(i)] = 0.f;
+  if (Xc.size(0) == 0)
+    return {torch::empty({0}, torch::TensorOptions().dtype(torch::kInt32).device(X.device())), out};
+  if (host) Xc = require_cuda_copy(Xc);
+  c10::cuda::CUDAGuard guard(Xc.device());
+  const int64_t n = Xc.size(0);
+  auto labels = torch::empty({n}, torch::TensorOptions().dtype(torch::kInt32).device(Xc.device()));
+  const size_t bytes = dbs_workspace_bytes(n, 1);
+  auto ws = alloc_ws(bytes, Xc.device());
+  cudaStream_t stream = at::cuda::getCurrentCUDAStream();
+  float ms[DBS_NUM_STAGES];
+  check_rc(dbs_dbscan2d_profile(Xc.data_ptr<float>(), n, eps, min_samples,
+                                labels.data_ptr<int32_t>(), ws.data_ptr(), bytes, stream, ms),
+           "dbscan2d_profile");
+  uint32_t st = 0;
+  check_rc(dbs_read_status(ws.data_ptr(), stream, &st), "dbscan2d_profile");
+  raise_if_failed(st);
+  for (int i = 0; i < DBS_NUM_STAGES; ++i) out[dbs_stage_name(i)] = ms[i];
+  if (host) labels = labels.to(torch::kCPU);
+  return {labels, out};
+}
+
+std::vector<torch::Tensor> dbscan2d_cuda_debug(torch::Tensor X, double eps, int64_t min_samples) {
+  TORCH_CHECK(X.dim() == 2 && X.size(0) > 0, "debug variant requires n > 0");
+  check_input(X, eps, min_samples);
+  TORCH_CHECK(X.is_cuda(), "X must be on CUDA");
+  auto Xc = X.contiguous();
+  c10::cuda::CUDAGuard guard(Xc.device());
+  const int64_t n = Xc.size(0);
+  auto dev = Xc.device();
+  auto i32 = torch::TensorOptions().dtype(torch::kInt32).device(dev);
+  auto labels = torch::empty({n}, i32);
+  auto keys = torch::empty({n}, torch::TensorOptions().dtype(torch::kInt64).device(dev));
+  auto perm = torch::empty({n}, i32);
+  auto xs = torch::empty({n}, Xc.options());
+  auto ys = torch::empty({n}, Xc.options());
+  auto is_core = torch::empty({n}, torch::TensorOptions().dtype(torch::kUInt8).device(dev));
+  auto cell_start = torch::empty({n + 1}, i32);
+  auto cluster_id = torch::empty({n}, i32);
+  auto uf = torch::empty({n}, i32);
+  auto pre = torch::empty({n}, i32);
+  auto fin = torch::empty({n}, i32);
+  const size_t bytes = dbs_workspace_bytes(n, 1);
+  auto ws = alloc_ws(bytes, dev);
+  cudaStream_t stream = at::cuda::getCurrentCUDAStream();
+  dbs_debug_buffers o;
+  o.keys_sorted = keys.data_ptr<int64_t>();
+  o.perm = perm.data_ptr<int32_t>();
+  o.xs = xs.data_ptr<float>();
+  o.ys = ys.data_ptr<float>();
+  o.is_core = is_core.data_ptr<uint8_t>();
+  o.cell_start = cell_start.data_ptr<int32_t>();
+  o.cluster_id_per_cell = cluster_id.data_ptr<int32_t>();
+  o.uf = uf.data_ptr<int32_t>();
+  o.sorted_labels_pre_border = pre.data_ptr<int32_t>();
+  o.sorted_labels_final = fin.data_ptr<int32_t>();
+  int64_t C = 0;
+  check_rc(dbs_dbscan2d_debug(Xc.data_ptr<float>(), n, eps, min_samples,
+                              labels.data_ptr<int32_t>(), ws.data_ptr(), bytes, stream, &o, &C),
+           "dbscan2d_cuda_debug");
+  uint32_t st = 0;
+  check_rc(dbs_read_status(ws.data_ptr(), stream, &st), "dbscan2d_cuda_debug");
+  raise_if_failed(st);
+  return {labels, keys, perm, xs, ys, is_core, cell_start.slice(0, 0, C + 1),
+          cluster_id.slice(0, 0, C), uf.slice(0, 0, C), pre, fin};
+}
+
+// Batched: X (N_total, 2) on CUDA; seg_offsets int64 (S+1), eps float64 (S),
+// min_samples int64 (S) as CPU tensors. Labels per cloud are numbered from 0.
+torch::Tensor dbscan2d_batched(torch::Tensor X, torch::Tensor seg_offsets, torch::Tensor eps,
+                               torch::Tensor min_samples) {
+  TORCH_CHECK(X.dim() == 2 && X.size(1) == 2, "X must have shape (N, 2)");
+  TORCH_CHECK(X.scalar_type() == torch::kFloat32, "X must be float32");
+  auto off = seg_offsets.to(torch::kCPU, torch::kInt64).contiguous();
+  auto ep = eps.to(torch::kCPU, torch::kFloat64).contiguous();
+  auto ms = min_samples.to(torch::kCPU, torch::kInt64).contiguous();
+  const int64_t S = ep.numel();
+  TORCH_CHECK(S >= 1, "at least one cloud is required");
+  TORCH_CHECK(S <= INT32_MAX, "too many clouds");
+  TORCH_CHECK(off.dim() == 1 && off.numel() == S + 1, "seg_offsets must have len(eps) + 1 entries");
+  TORCH_CHECK(ms.numel() == S, "min_samples must have one entry per cloud");
+  const int64_t* o = off.data_ptr<int64_t>();
+  TORCH_CHECK(o[0] == 0 && o[S] == X.size(0), "seg_offsets must start at 0 and end at N");
+  const double* e = ep.data_ptr<double>();
+  const int64_t* m = ms.data_ptr<int64_t>();
+  for (int64_t s = 0; s < S; ++s) {
+    TORCH_CHECK(o[s + 1] >= o[s], "seg_offsets must be non-decreasing");
+    TORCH_CHECK(e[s] > 0.0, "eps must be > 0");
+    TORCH_CHECK(m[s] >= 1, "min_samples must be >= 1");
+  }
+  const bool host = !X.is_cuda();
+  torch::Tensor Xc = X.contiguous();
+  if (Xc.size(0) == 0) return torch::empty({0}, torch::TensorOptions().dtype(torch::kInt32).device(X.device()));
+  if (host) Xc = require_cuda_copy(Xc);
+  c10::cuda::CUDAGuard guard(Xc.device());
+  const int64_t n = Xc.size(0);
+  auto labels = torch::empty({n}, torch::TensorOptions().dtype(torch::kInt32).device(Xc.device()));
+  if (!capturing(at::cuda::getCurrentCUDAStream())) drain(false);
+  const size_t bytes = dbs_workspace_bytes(n, (int32_t)S);
+  auto ws = alloc_ws(bytes, Xc.device());
+  cudaStream_t stream = at::cuda::getCurrentCUDAStream();
+  check_rc(dbs_dbscan2d_batched(Xc.data_ptr<float>(), o, e, m, (int32_t)S,
+                                labels.data_ptr<int32_t>(), ws.data_ptr(), bytes, stream),
+           "dbscan2d_batched");
+  after_launch(ws, stream);
+  if (host) labels = labels.to(torch::kCPU);
+  return labels;
+}
+
+// Graph-capturable batched run on caller-owned buffers: every argument is a
+// CUDA tensor that stays alive across replays. params: uint8 (S*16) filled by
+// fill_seg_params; ws: uint8 of workspace_bytes(N, S).
+void dbscan2d_batched_into(torch::Tensor X, torch::Tensor seg_offsets_dev, torch::Tensor params_dev,
+                           torch::Tensor labels, torch::Tensor ws) {
+  TORCH_CHECK(X.is_cuda() && seg_offsets_dev.is_cuda() && params_dev.is_cuda() && labels.is_cuda() &&
+                  ws.is_cuda(),
+              "all tensors must be on CUDA");
+  TORCH_CHECK(X.is_contiguous() && X.scalar_type() == torch::kFloat32 && X.dim() == 2 && X.size(1) == 2,
+              "X must be a contiguous float32 (N, 2) tensor");
+  TORCH_CHECK(seg_offsets_dev.scalar_type() == torch::kInt64, "seg_offsets must be int64");
+  TORCH_CHECK(labels.scalar_type() == torch::kInt32 && labels.numel() == X.size(0), "labels must be int32 (N,)");
+  const int64_t S = seg_offsets_dev.numel() - 1;
+  TORCH_CHECK(S >= 1 && params_dev.numel() == S * 16, "params must hold 16 bytes per cloud");
+  c10::cuda::CUDAGuard guard(X.device());
+  cudaStream_t stream = at::cuda::getCurrentCUDAStream();
+  check_rc(dbs_dbscan2d_batched_device(X.data_ptr<float>(), X.size(0), (int32_t)S,
+                                       seg_offsets_dev.data_ptr<int64_t>(), params_dev.data_ptr(),
+                                       labels.data_ptr<int32_t>(), ws.data_ptr(), ws.numel(), stream),
+           "dbscan2d_batched_into");
+}
+
+torch::Tensor fill_seg_params(torch::Tensor eps, torch::Tensor min_samples) {
+  auto ep = eps.to(torch::kCPU, torch::kFloat64).contiguous();
+  auto ms = min_samples.to(torch::kCPU, torch::kInt64).contiguous();
+  TORCH_CHECK(ep.numel() == ms.numel() && ep.numel() >= 1, "eps and min_samples must match");
+  auto out = torch::empty({ep.numel() * 16}, torch::TensorOptions().dtype(torch::kUInt8));
+  check_rc(dbs_fill_seg_params(ep.data_ptr<double>(), ms.data_ptr<int64_t>(), (int32_t)ep.numel(),
+                               out.data_ptr()),
+           "fill_seg_params");
+  return out;
+}
+
+int64_t workspace_bytes(int64_t n, int64_t nseg) {
+  return (int64_t)dbs_workspace_bytes(n, (int32_t)nseg);
+}
+
+int64_t read_status(torch::Tensor ws) {
+  TORCH_CHECK(ws.is_cuda(), "ws must be on CUDA");
+  uint32_t st = 0;
+  check_rc(dbs_read_status(ws.data_ptr(), at::cuda::getCurrentCUDAStream(), &st), "read_status");
+  return st;
+}
+
+void check_status() { drain(true); }
+
+// Plain call that also reports the pipeline's shape (synchronises): labels,
+// {num_cells, key_bits, passes, key_bytes}.
+std::pair<torch::Tensor, std::map<std::string, int64_t>> dbscan2d_info(torch::Tensor X, double eps,
+                                                                       int64_t min_samples) {
+  check_input(X, eps, min_samples);
+  TORCH_CHECK(X.is_cuda() && X.size(0) > 0, "dbscan2d_info needs a non-empty CUDA tensor");
+  auto Xc = X.contiguous();
+  c10::cuda::CUDAGuard guard(Xc.device());
+  const int64_t n = Xc.size(0);
+  auto labels = torch::empty({n}, torch::TensorOptions().dtype(torch::kInt32).device(Xc.device()));
+  const size_t bytes = dbs_workspace_bytes(n, 1);
+  auto ws = alloc_ws(bytes, Xc.device());
+  cudaStream_t stream = at::cuda::getCurrentCUDAStream();
+  check_rc(dbs_dbscan2d(Xc.data_ptr<float>(), n, eps, min_samples, labels.data_ptr<int32_t>(),
+                        ws.data_ptr(), bytes, stream),
+           "dbscan2d_info");
+  int64_t cells = 0;
+  int32_t bits = 0, passes = 0, kb = 0;
+  check_rc(dbs_read_plan(ws.data_ptr(), stream, &cells, &bits, &passes, &kb), "dbscan2d_info");
+  uint32_t st = 0;
+  check_rc(dbs_read_status(ws.data_ptr(), stream, &st), "dbscan2d_info");
+  raise_if_failed(st);
+  std::map<std::string, int64_t> info{{"num_cells", cells}, {"key_bits", bits},
+                                      {"passes", passes}, {"key_bytes", kb}};
+  return {labels, info};
+}
+
+PYBIND11_MODULE(_C, m) {
+  m.doc() = "B200-native DBSCAN (2D, grid-hashed): sm_100a kernels behind a C-ABI.";
+  m.def("dbscan2d", &dbscan2d, pybind11::arg("X"), pybind11::arg("eps"), pybind11::arg("min_samples"),
+        "Run DBSCAN on (N, 2) float32 tensor. Returns int32 labels (-1 = noise) on X's device. "
+        "Computes on CUDA; a CPU tensor is copied to the current CUDA device and back.");
+  m.def("dbscan2d_profile", &dbscan2d_profile, pybind11::arg("X"), pybind11::arg("eps"),
+        pybind11::arg("min_samples"),
+        "Profile variant: returns (labels, {stage_name: ms}) with GPU time per reference stage.");
+  m.def("dbscan2d_cuda_debug", &dbscan2d_cuda_debug, pybind11::arg("X"), pybind11::arg("eps"),
+        pybind11::arg("min_samples"),
+        "Debug variant: the reference's 11 per-stage intermediate tensors. Not public API.");
+  m.def("dbscan2d_batched", &dbscan2d_batched, pybind11::arg("X"), pybind11::arg("seg_offsets"),
+        pybind11::arg("eps"), pybind11::arg("min_samples"),
+        "Many clouds in one pipeline run; labels numbered per cloud.");
+  m.def("dbscan2d_batched_into", &dbscan2d_batched_into, pybind11::arg("X"),
+        pybind11::arg("seg_offsets"), pybind11::arg("params"), pybind11::arg("labels"),
+        pybind11::arg("ws"), "Batched run on device-resident buffers (CUDA-graph capturable).");
+  m.def("fill_seg_params", &fill_seg_params, pybind11::arg("eps"), pybind11::arg("min_samples"));
+  m.def("workspace_bytes", &workspace_bytes, pybind11::arg("n"), pybind11::arg("nseg") = 1);
+  m.def("read_status", &read_status, pybind11::arg("ws"));
+  m.def("dbscan2d_info", &dbscan2d_info, pybind11::arg("X"), pybind11::arg("eps"),
+        pybind11::arg("min_samples"), "Labels plus the pipeline's shape (cells, key bits, passes).");
+  m.def("check_status", &check_status,
+        "Wait for every pending call and raise RuntimeError if one recorded a device failure.");
+}

@@ -1,0 +1,141 @@
+/*
+ * dbscan_b200.h -- C-ABI of the sm_100a grid-hashed 2D DBSCAN library
+ * (libdbscan_b200.so).
+ *
+ * Drop-in boundary for the GPU path of ryanirl/dbscan-torch v0.2.0. Each
+ * entry point below replaces one function of the reference's CUDA translation
+ * unit (csrc/cuda/dbscan_cuda.cu) that its pybind module binds through
+ * csrc/extension.cpp; the torch extension of this repository (_C) is a thin
+ * C++ layer that validates tensors exactly like extension.cpp:26-31 and calls
+ * these functions. No torch, thrust or CUB types cross this boundary: plain
+ * pointers, sizes and a cudaStream_t passed as void*.
+ *
+ * Conventions
+ *   - X is float32 (n, 2) row-major (AoS x, y), device memory unless noted.
+ *   - labels are int32 (n,), -1 = noise, else a cluster id in [0, k) numbered
+ *     exactly like the reference CUDA path (rank of each cluster's smallest
+ *     cell in ascending unsigned cell-key order).
+ *   - eps and min_samples follow dbscan_cuda.cu:547-550: fl_eps = (float)eps,
+ *     inv_r = sqrtf(2)/fl_eps, eps_sq = fl_eps*fl_eps, ms = (int32)min_samples.
+ *   - ws is a caller-owned device workspace of at least
+ *     dbs_workspace_bytes(n, nseg) bytes, 256-byte aligned. The library never
+ *     allocates device memory; calls on one workspace must not overlap.
+ *   - All work is enqueued on `stream` (a cudaStream_t; NULL = legacy default
+ *     stream). Unless stated otherwise an entry point does not synchronise:
+ *     the enqueue sequence holds no host read-back, so it can be captured in
+ *     a CUDA graph. Device-side failures (a bounded wait that ran out) are
+ *     recorded in the workspace and read with dbs_read_status().
+ *   - Return value: DBS_OK or a DBS_ERR_* code (see dbs_strerror()).
+ */
+#ifndef DBSCAN_B200_H_
+#define DBSCAN_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DBS_OK 0
+#define DBS_ERR_INVALID 1       /* bad argument: shape, eps <= 0, min_samples < 1, n < 0 */
+#define DBS_ERR_WORKSPACE 2     /* ws NULL, misaligned or smaller than required */
+#define DBS_ERR_TOO_LARGE 3     /* n >= 2^31 (the reference indexes points with int32) */
+#define DBS_ERR_CUDA 4          /* a CUDA runtime call failed */
+#define DBS_ERR_DEVICE 5        /* device status word non-zero (see dbs_read_status) */
+
+/* Device status bits (dbs_read_status). */
+#define DBS_STATUS_LOOKBACK 1u  /* a decoupled look-back wait reached its cap */
+#define DBS_STATUS_FIND 2u      /* a union-find walk reached its cap */
+#define DBS_STATUS_KEYSPACE 4u  /* batched cell-key ranges overflowed 64 bits */
+
+#define DBS_NUM_STAGES 10
+
+/* Bytes of device workspace for nseg clouds holding n_total points. */
+size_t dbs_workspace_bytes(int64_t n_total, int32_t nseg);
+
+/* Plain call. Replaces dbscan2d_cuda (dbscan_cuda.cu:752-755), bound as
+ * _C.dbscan2d (extension.cpp:33-45, 67-70). n == 0 is a no-op. */
+int dbs_dbscan2d(const float* X, int64_t n, double eps, int64_t min_samples,
+                 int32_t* labels, void* ws, size_t ws_bytes, void* stream);
+
+/* Profile call. Replaces dbscan2d_cuda_profile (dbscan_cuda.cu:760-770),
+ * bound as _C.dbscan2d_profile (extension.cpp:52-63, 71-74). Fills
+ * stage_ms[DBS_NUM_STAGES] with the GPU time of each of the reference's ten
+ * stages (names from dbs_stage_name()). Synchronises the stream. */
+int dbs_dbscan2d_profile(const float* X, int64_t n, double eps, int64_t min_samples,
+                         int32_t* labels, void* ws, size_t ws_bytes, void* stream,
+                         float* stage_ms);
+
+/* Debug call. Replaces dbscan2d_cuda_debug (dbscan_cuda.cu:790-800), bound as
+ * _C.dbscan2d_cuda_debug (extension.cpp:76-79). Writes the reference's
+ * per-stage intermediates (layout dbscan_cuda.cu:777-789) into caller device
+ * buffers; cell-sized buffers need capacity n (cell_start n + 1). Any pointer
+ * may be NULL. Synchronises the stream and returns num_cells in *num_cells. */
+typedef struct dbs_debug_buffers {
+  int64_t* keys_sorted;          /* (n) u64-packed (u32)kx << 32 | (u32)ky, sorted */
+  int32_t* perm;                 /* (n) sorted position -> input index */
+  float* xs;                     /* (n) sorted x */
+  float* ys;                     /* (n) sorted y */
+  uint8_t* is_core;              /* (n) sorted order */
+  int32_t* cell_start;           /* (num_cells + 1) */
+  int32_t* cluster_id_per_cell;  /* (num_cells) */
+  int32_t* uf;                   /* (num_cells) flattened roots */
+  int32_t* sorted_labels_pre_border; /* (n) core labels in sorted order */
+  int32_t* sorted_labels_final;  /* (n) final labels in sorted order */
+} dbs_debug_buffers;
+
+int dbs_dbscan2d_debug(const float* X, int64_t n, double eps, int64_t min_samples,
+                       int32_t* labels, void* ws, size_t ws_bytes, void* stream,
+                       const dbs_debug_buffers* out, int64_t* num_cells);
+
+/* Batched call (no counterpart in the reference; the reference handles one
+ * cloud per dbscan2d call). nseg clouds are concatenated in X; cloud s owns
+ * rows [seg_offsets[s], seg_offsets[s+1]) and has its own eps[s] and
+ * min_samples[s]. seg_offsets, eps and min_samples are HOST arrays; labels
+ * of cloud s land in the same rows of `labels`, each cloud numbered from 0
+ * exactly as a plain call on that cloud alone. One pipeline launch sequence
+ * covers every cloud. */
+int dbs_dbscan2d_batched(const float* X, const int64_t* seg_offsets, const double* eps,
+                         const int64_t* min_samples, int32_t nseg, int32_t* labels,
+                         void* ws, size_t ws_bytes, void* stream);
+
+/* Batched call with the per-cloud table already on the device, for CUDA
+ * graph capture. seg_offsets_dev: int64 (nseg + 1); seg_params_dev: nseg
+ * records of {float inv_r, float eps_sq, int32 ms, int32 pad} computed as in
+ * the conventions above (dbs_fill_seg_params fills such a table on the host). */
+int dbs_dbscan2d_batched_device(const float* X, int64_t n_total, int32_t nseg,
+                                const int64_t* seg_offsets_dev, const void* seg_params_dev,
+                                int32_t* labels, void* ws, size_t ws_bytes, void* stream);
+
+/* Host helper: fills nseg 16-byte parameter records (see above). */
+int dbs_fill_seg_params(const double* eps, const int64_t* min_samples, int32_t nseg,
+                        void* params_host);
+
+/* Host-buffer call: X and labels in HOST memory (pinned for asynchronous
+ * copies). Copies in, runs the plain pipeline, copies out and synchronises.
+ * ws must hold dbs_host_workspace_bytes(n). This is the end-to-end form of
+ * _C.dbscan2d for a CPU tensor. */
+size_t dbs_host_workspace_bytes(int64_t n);
+int dbs_dbscan2d_host(const float* X_host, int64_t n, double eps, int64_t min_samples,
+                      int32_t* labels_host, void* ws, size_t ws_bytes, void* stream);
+
+/* Synchronises the stream and returns the device status word of the last
+ * call on this workspace (0 = no failure; DBS_STATUS_* bits otherwise). */
+int dbs_read_status(const void* ws, void* stream, uint32_t* status);
+
+/* Shape of the last call on this workspace, read after synchronising the
+ * stream: number of cells (distinct occupied grid cells over all clouds),
+ * significant bits of the compacted cell keys, radix passes that ran, and
+ * bytes per stored key (4 or 8). Any output pointer may be NULL. */
+int dbs_read_plan(const void* ws, void* stream, int64_t* num_cells, int32_t* key_bits,
+                  int32_t* passes, int32_t* key_bytes);
+
+const char* dbs_strerror(int code);
+const char* dbs_stage_name(int stage);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DBSCAN_B200_H_ */

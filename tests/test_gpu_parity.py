@@ -1,0 +1,89 @@
+"""Raw-label parity of the sm_100a pipeline with the oracle (and with the
+reference's own CUDA build when it is present in oracle/_ref/cuda).
+
+Bit-exact: labels are integers, so equality is exact -- cluster numbering,
+noise and the (d2, perm[j]) border tie rule included. The debug entry point
+is compared intermediate by intermediate (layout of dbscan_cuda.cu:777-789).
+"""
+
+import numpy as np
+import pytest
+import torch
+
+import datasets
+import oracle
+import refmod
+from dbscan_torch import _C, dbscan2d, dbscan2d_batched
+
+pytestmark = pytest.mark.gpu
+
+CASES = datasets.parity_cases()
+IDS = [c[0] for c in CASES]
+
+
+@pytest.mark.parametrize("name,X,eps,ms", CASES, ids=IDS)
+def test_labels_match_oracle(name, X, eps, ms):
+    ours = dbscan2d(torch.from_numpy(X).cuda(), eps, ms).cpu().numpy()
+    ref = oracle.dbscan2d(X, eps, ms)
+    diff = np.flatnonzero(ours != ref)
+    assert diff.size == 0, f"{name}: {diff.size}/{X.shape[0]} labels differ, first at {diff[:10]}"
+
+
+@pytest.mark.parametrize("name,X,eps,ms", CASES[:12], ids=IDS[:12])
+def test_debug_intermediates_match_oracle(name, X, eps, ms):
+    out = _C.dbscan2d_cuda_debug(torch.from_numpy(X).cuda(), eps, ms)
+    o = oracle.dbscan2d(X, eps, ms, debug=True)
+    names = ["labels", "keys_sorted", "perm", "xs", "ys", "is_core", "cell_start",
+             "cluster_id_per_cell", "uf", "sorted_labels_pre_border", "sorted_labels_final"]
+    for k, t in zip(names, out):
+        a = t.cpu().numpy()
+        b = o[k]
+        if k == "keys_sorted":
+            b = b.view(np.int64)
+        assert a.shape == b.shape, f"{name}/{k}: shape {a.shape} vs {b.shape}"
+        assert np.array_equal(a, b), f"{name}/{k}: {(a != b).sum()} entries differ"
+
+
+def test_repeated_runs_bit_identical():
+    for make in (datasets.dense_overlapping_blobs, datasets.near_percolation_uniform):
+        X = torch.from_numpy(make(50_000, 0)).cuda()
+        first = dbscan2d(X, 0.5, 5)
+        for _ in range(4):
+            assert torch.equal(first, dbscan2d(X, 0.5, 5))
+
+
+def test_batched_equals_plain():
+    rng = np.random.default_rng(5)
+    clouds, eps, ms = [], [], []
+    for k in range(37):
+        n = int(rng.integers(1, 3000)) if k % 5 else 0
+        clouds.append(datasets.dense_overlapping_blobs(max(n, 0), k) if n else np.zeros((0, 2), np.float32))
+        eps.append(float(rng.uniform(0.2, 1.0)))
+        ms.append(int(rng.integers(1, 33)))
+    off = np.concatenate([[0], np.cumsum([c.shape[0] for c in clouds])])
+    X = torch.from_numpy(np.concatenate(clouds)).cuda()
+    lab = dbscan2d_batched(X, off, eps, ms).cpu().numpy()
+    for s, c in enumerate(clouds):
+        if c.shape[0] == 0:
+            continue
+        want = oracle.dbscan2d(c, eps[s], ms[s])
+        got = lab[off[s]:off[s + 1]]
+        assert np.array_equal(got, want), f"cloud {s}: {(got != want).sum()} labels differ"
+
+
+def test_cpu_tensor_roundtrip():
+    X = datasets.three_blobs()
+    lab = dbscan2d(torch.from_numpy(X), 1.0, 5)
+    assert lab.device.type == "cpu" and lab.dtype == torch.int32
+    assert np.array_equal(lab.numpy(), oracle.dbscan2d(X, 1.0, 5))
+
+
+@pytest.mark.parametrize("name,X,eps,ms", CASES, ids=IDS)
+def test_labels_match_reference_cuda(name, X, eps, ms):
+    ref = refmod.load("cuda")
+    if ref is None:
+        pytest.skip("reference CUDA build not present in oracle/_ref/cuda")
+    want = ref.dbscan2d(torch.from_numpy(X).cuda(), eps, ms).cpu().numpy()
+    ours = dbscan2d(torch.from_numpy(X).cuda(), eps, ms).cpu().numpy()
+    diff = np.flatnonzero(ours != want)
+    assert diff.size == 0, f"{name}: {diff.size} labels differ from the reference CUDA path"
