@@ -55,6 +55,7 @@ size_t carve(int64_t n, int32_t nseg, char* base, Plan* p) {
   q.sweep_status[1] = cv.take<unsigned long long>((size_t)sweep_tiles * kRadix);
   q.rle_status = cv.take<unsigned long long>((size_t)scan_tiles);
   q.ids_status = cv.take<unsigned long long>((size_t)scan_tiles);
+  q.point_cell = cv.take<int32_t>(N);
   q.cell_start = cv.take<int32_t>(N + 1);
   q.cell_key = cv.take<uint64_t>(N);
   q.cell_seg = cv.take<int32_t>(N);

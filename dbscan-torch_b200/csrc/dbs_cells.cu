@@ -12,9 +12,9 @@
 // also record each cell in a dense map indexed by the compacted key, so
 // neighbour lookup is one load instead of a binary search.
 //
-// k_cell_prep gives each cell one warp: the lanes reduce the bounding box of
-// the cell's points and lanes 0..24 resolve the 25 offsets of the 5x5
-// stencil in the reference's order (off = (dx+2)*5 + (dy+2)).
+// k_cell_prep gives each cell one thread: it folds the bounding box of the
+// cell's points and resolves the 25 offsets of the 5x5 stencil in the
+// reference's order (off = (dx+2)*5 + (dy+2)).
 #include "dbs_internal.cuh"
 
 namespace dbs {
@@ -80,24 +80,26 @@ __device__ __forceinline__ void rle_body(const Plan& p, K* s_keys, uint32_t* s_w
       }
     }
     __syncthreads();
+    // c: cells started before this thread's first item.
     uint32_t c = (uint32_t)*s_excl + s_warp[warp] + x - cnt;
-    if (flags) {
-      int32_t seg = seg_of(p, base + j0);
+    int32_t seg = flags ? seg_of(p, base + j0) : 0;
 #pragma unroll 1
-      for (int k = 0; k < kScanItems; ++k) {
-        if (!((flags >> k) & 1u)) continue;
-        const int64_t i = base + j0 + k;
+    for (int k = 0; k < kScanItems && j0 + k < valid; ++k) {
+      const int64_t i = base + j0 + k;
+      if ((flags >> k) & 1u) {
         const uint64_t key = (uint64_t)s_keys[j0 + k + 1];
         while (i >= p.seg_off[seg + 1]) ++seg;
-        if ((int64_t)c >= n) break;  // only after a failed look-back
-        p.cell_start[c] = (int32_t)i;
-        p.cell_key[c] = key;
-        p.cell_seg[c] = seg;
-        if (i == p.seg_off[seg]) p.seg_info[seg].cell_begin = (int32_t)c;
-        const int64_t mb = p.seg_info[seg].map_base;
-        if (mb >= 0) p.cell_map[mb + (int64_t)(key - p.seg_info[seg].base)] = (int32_t)c;
+        if ((int64_t)c < n) {  // (c >= n only after a failed look-back)
+          p.cell_start[c] = (int32_t)i;
+          p.cell_key[c] = key;
+          p.cell_seg[c] = seg;
+          if (i == p.seg_off[seg]) p.seg_info[seg].cell_begin = (int32_t)c;
+          const int64_t mb = p.seg_info[seg].map_base;
+          if (mb >= 0) p.cell_map[mb + (int64_t)(key - p.seg_info[seg].base)] = (int32_t)c;
+        }
         ++c;
       }
+      p.point_cell[i] = (int32_t)max((int64_t)0, min((int64_t)c - 1, n - 1));
     }
     __syncthreads();
   }
@@ -115,9 +117,10 @@ __global__ void __launch_bounds__(kScanThreads) k_rle(Plan p) {
 }
 
 // ------------------------------------------------------------ k_cell_prep
+// Cell index of compacted coordinates (gx, gy) of cloud s, or -1.
 __device__ __forceinline__ int32_t find_cell(const Plan& p, const SegInfo& g, int32_t s,
                                              uint64_t gx, uint64_t gy, uint32_t num_cells) {
-  const uint64_t local = gx * g.wy + gy;
+  const uint64_t local = (gx << g.ysh) + gy;
   if (g.map_base >= 0) return p.cell_map[g.map_base + (int64_t)local];
   const uint64_t target = g.base + local;
   // Binary search over the cloud's cells (at most min(range, points) cells).
@@ -132,57 +135,82 @@ __device__ __forceinline__ int32_t find_cell(const Plan& p, const SegInfo& g, in
   return -1;
 }
 
+constexpr int32_t kBigCell = 64;  // cells above this size reduce their box per warp
+
+// One thread per cell: bounding box of the cell's points and the 25-entry
+// neighbour row. Cells larger than kBigCell points get their box from the
+// whole warp afterwards (a 2M-point cell would otherwise be one thread's
+// serial loop).
 __global__ void __launch_bounds__(kCellThreads) k_cell_prep(Plan p) {
   const uint32_t full = 0xffffffffu;
   const uint32_t lane = lane_id();
   const uint32_t C = p.desc->num_cells;
-  while (true) {
-    uint32_t c = 0;
-    if (lane == 0) c = atomicAdd(&p.desc->ctr[kCtrPrep], 1u);
-    c = __shfl_sync(full, c, 0);
-    if (c >= C) break;
-    const int32_t s0 = p.cell_start[c], s1 = p.cell_start[c + 1];
-    // Bounding box. A one-point cell keeps its raw coordinates (the
-    // reference seeds the fold with xs[s] and folds fminf/fmaxf over the
-    // rest, which flushes subnormals only when there is a rest).
-    float xmin = INFINITY, xmax = -INFINITY, ymin = INFINITY, ymax = -INFINITY;
-    for (int32_t i = s0 + lane; i < s1; i += 32) {
-      const float2 v = p.xy[i];
-      xmin = fminf(xmin, v.x); xmax = fmaxf(xmax, v.x);
-      ymin = fminf(ymin, v.y); ymax = fmaxf(ymax, v.y);
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      xmin = fminf(xmin, __shfl_xor_sync(full, xmin, o));
-      xmax = fmaxf(xmax, __shfl_xor_sync(full, xmax, o));
-      ymin = fminf(ymin, __shfl_xor_sync(full, ymin, o));
-      ymax = fmaxf(ymax, __shfl_xor_sync(full, ymax, o));
-    }
-    if (lane == 0) {
-      if (s1 - s0 == 1) {
-        const float2 v = p.xy[s0];
-        p.bbox[c] = make_float4(v.x, v.x, v.y, v.y);
-      } else {
-        p.bbox[c] = make_float4(xmin, xmax, ymin, ymax);
+  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t wbase = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; wbase < C;
+       wbase += warps * 32) {
+    const uint32_t c = wbase + lane;
+    const bool valid = c < C;
+    int32_t s0 = 0, s1 = 0;
+    if (valid) { s0 = p.cell_start[c]; s1 = p.cell_start[c + 1]; }
+    const bool big = valid && (s1 - s0) > kBigCell;
+    if (valid && !big) {
+      // A one-point cell keeps its raw coordinates: the reference seeds the
+      // fold with xs[s] and flushes subnormals only through fminf/fmaxf.
+      float2 v = p.xy[s0];
+      float4 b = make_float4(v.x, v.x, v.y, v.y);
+      if (s1 - s0 > 1) {
+        b = make_float4(INFINITY, -INFINITY, INFINITY, -INFINITY);
+        for (int32_t i = s0; i < s1; ++i) {
+          v = p.xy[i];
+          b.x = fminf(b.x, v.x); b.y = fmaxf(b.y, v.x);
+          b.z = fminf(b.z, v.y); b.w = fmaxf(b.w, v.y);
+        }
       }
+      p.bbox[c] = b;
     }
-    // Neighbour table.
-    if (lane < kNgh) {
-      const int32_t s = p.cell_seg[c];
-      const SegInfo& g = p.seg_info[s];
-      const uint64_t local = p.cell_key[c] - g.base;
-      const uint64_t gx = local / g.wy;
-      const uint64_t gy = local - gx * g.wy;
-      const int32_t kx = expand_axis(gx, g.bx, g.px);
-      const int32_t ky = expand_axis(gy, g.by, g.py);
-      const int32_t dx = (int32_t)(lane / 5) - 2, dy = (int32_t)(lane % 5) - 2;
-      const int32_t nkx = (int32_t)((uint32_t)kx + (uint32_t)dx);
-      const int32_t nky = (int32_t)((uint32_t)ky + (uint32_t)dy);
-      const uint64_t ngx = compact_axis(nkx, g.bx, g.px);
-      const uint64_t ngy = compact_axis(nky, g.by, g.py);
-      int32_t r = -1;
-      if (ngx != ~0ull && ngy != ~0ull) r = find_cell(p, g, s, ngx, ngy, C);
-      p.ngh[(int64_t)c * kNgh + lane] = r;
+    uint32_t bm = __ballot_sync(full, big);
+    while (bm) {
+      const int l = __ffs(bm) - 1;
+      bm &= bm - 1;
+      const int32_t b0 = __shfl_sync(full, s0, l), b1 = __shfl_sync(full, s1, l);
+      float xmin = INFINITY, xmax = -INFINITY, ymin = INFINITY, ymax = -INFINITY;
+      for (int32_t i = b0 + lane; i < b1; i += 32) {
+        const float2 v = p.xy[i];
+        xmin = fminf(xmin, v.x); xmax = fmaxf(xmax, v.x);
+        ymin = fminf(ymin, v.y); ymax = fmaxf(ymax, v.y);
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        xmin = fminf(xmin, __shfl_xor_sync(full, xmin, o));
+        xmax = fmaxf(xmax, __shfl_xor_sync(full, xmax, o));
+        ymin = fminf(ymin, __shfl_xor_sync(full, ymin, o));
+        ymax = fmaxf(ymax, __shfl_xor_sync(full, ymax, o));
+      }
+      if ((int)lane == l) p.bbox[c] = make_float4(xmin, xmax, ymin, ymax);
+    }
+    if (!valid) continue;
+    // Neighbour row, off = (dx+2)*5 + (dy+2) as in the reference.
+    const int32_t s = p.cell_seg[c];
+    const SegInfo& g = p.seg_info[s];
+    const uint64_t local = p.cell_key[c] - g.base;
+    const uint64_t gx = local >> g.ysh;
+    const uint64_t gy = local & ((1ull << g.ysh) - 1ull);
+    const int32_t kx = expand_axis(gx, g.bx, g.px);
+    const int32_t ky = expand_axis(gy, g.by, g.py);
+    uint64_t ngy[5];
+#pragma unroll
+    for (int dy = 0; dy < 5; ++dy)
+      ngy[dy] = compact_axis((int32_t)((uint32_t)ky + (uint32_t)(dy - 2)), g.by, g.py);
+    int32_t* row = p.ngh + (int64_t)c * kNgh;
+#pragma unroll
+    for (int dx = 0; dx < 5; ++dx) {
+      const uint64_t ngx = compact_axis((int32_t)((uint32_t)kx + (uint32_t)(dx - 2)), g.bx, g.px);
+#pragma unroll
+      for (int dy = 0; dy < 5; ++dy) {
+        int32_t r = -1;
+        if (ngx != ~0ull && ngy[dy] != ~0ull) r = find_cell(p, g, s, ngx, ngy[dy], C);
+        row[dx * 5 + dy] = r;
+      }
     }
   }
 }
@@ -196,7 +224,7 @@ cudaError_t launch_rle(const Plan& p, cudaStream_t s) {
 }
 
 cudaError_t launch_cell_prep(const Plan& p, cudaStream_t s) {
-  k_cell_prep<<<p.num_sms * 8, kCellThreads, 0, s>>>(p);
+  k_cell_prep<<<p.num_sms * 4, kCellThreads, 0, s>>>(p);
   return cudaGetLastError();
 }
 

@@ -7,20 +7,17 @@
 //   thrust::exclusive_scan :698-701, k_cluster_id_per_cell :392-404,
 //   k_core_labels :409-417, k_border_assign :427-470, k_unpermute :475-481.
 //
-// Every cell-level kernel gives one warp to one cell (cells taken in
-// ascending order from an atomic counter). The 5x5 neighbourhood of a cell
-// is flattened into one list of candidate points: lanes hold the 24 (or 25)
-// neighbour cells, a warp scan of their sizes gives each lane's slice, and
-// each step the 32 lanes test 32 candidates against one query point at a
-// time with ballots. The per-(query, neighbour-cell) bounding-box prune of
-// the reference is kept exactly (a bit mask per query), so every pair the
+// Core marking and labelling run one thread per sorted point, so the threads
+// of a warp are consecutive points, mostly of one cell: the neighbour row,
+// boxes and candidate points they read are the same addresses. Union-find
+// gives one warp to one core cell and one lane to each stencil neighbour.
+// The reference's bounding-box prunes are kept exactly, so every pair the
 // reference tests is tested with the same arithmetic and the same verdict.
 #include "dbs_internal.cuh"
 
 namespace dbs {
 
 constexpr uint32_t kFull = 0xffffffffu;
-constexpr int kWarpsPerBlock = kCellThreads / 32;
 
 __device__ __forceinline__ uint32_t next_cell(uint32_t* ctr) {
   uint32_t c = 0;
@@ -28,109 +25,62 @@ __device__ __forceinline__ uint32_t next_cell(uint32_t* ctr) {
   return __shfl_sync(kFull, c, 0);
 }
 
-// Smallest lane l with pre[l] > f (pre: inclusive prefix, 32 entries).
-__device__ __forceinline__ int slice_of(const int32_t* pre, int32_t f) {
-  int lo = 0;
-#pragma unroll
-  for (int step = 16; step > 0; step >>= 1)
-    if (pre[lo + step - 1] <= f) lo += step;
-  return lo;
-}
-
-// Warp inclusive scan.
-__device__ __forceinline__ int32_t warp_incl_scan(int32_t v) {
-  const uint32_t lane = lane_id();
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const int32_t y = __shfl_up_sync(kFull, v, o);
-    if (lane >= (uint32_t)o) v += y;
-  }
-  return v;
-}
-
 // ----------------------------------------------------------------- k_core
-// Core flag of every point and the cell status. Cells with >= ms points are
-// core wholesale (k_core_pass1). Otherwise each point counts its own cell
-// wholesale (the reference never distance-tests the centre cell, :231-233)
-// plus the points within eps in the other 24 cells that survive the
-// point-box prune (:235-240).
+// Core flag of every sorted point, one thread per point. A point of a cell
+// with >= ms points is core wholesale (k_core_pass1). Otherwise it counts its
+// own cell wholesale (the reference never distance-tests the centre cell,
+// :231-233) plus the points within eps of the other 24 stencil cells that
+// survive the point-box prune (:235-240), stopping once the count reaches ms.
+// Threads of one warp are consecutive points, mostly of one cell, so the
+// neighbour row, boxes and candidate points are shared loads.
 __global__ void __launch_bounds__(kCellThreads) k_core(Plan p) {
-  __shared__ int32_t s_pre[kWarpsPerBlock][32];
-  __shared__ int32_t s_off[kWarpsPerBlock][32];
-  const uint32_t lane = lane_id();
-  const uint32_t w = threadIdx.x >> 5;
-  const uint32_t C = p.desc->num_cells;
-  while (true) {
-    const uint32_t c = next_cell(&p.desc->ctr[kCtrCore]);
-    if (c >= C) break;
+  const int64_t n = p.n;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t c = p.point_cell[i];
     const int32_t st0 = p.cell_start[c], st1 = p.cell_start[c + 1];
-    const int32_t npts = st1 - st0;
     const SegParam sp = p.seg_param[p.cell_seg[c]];
     const int32_t ms = sp.ms;
+    int32_t cnt = st1 - st0;
+    if (cnt >= ms) { p.is_core[i] = 1; continue; }
     const float eps_sq = sp.eps_sq;
-    if (lane == 0) p.uf[c] = (int32_t)c;
-    if (npts >= ms) {
-      for (int32_t i = st0 + lane; i < st1; i += 32) p.is_core[i] = 1;
-      if (lane == 0) p.cell_status[c] = 2;
-      continue;
-    }
-    int32_t nb = -1, sz = 0, cs0 = 0;
-    float4 bb = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (lane < kNgh && lane != 12) {
-      nb = p.ngh[(int64_t)c * kNgh + lane];
-      if (nb >= 0) {
-        cs0 = p.cell_start[nb];
-        sz = p.cell_start[nb + 1] - cs0;
-        bb = p.bbox[nb];
+    const float2 q = p.xy[i];
+    const int32_t* row = p.ngh + (int64_t)c * kNgh;
+    for (int off = 0; off < kNgh && cnt < ms; ++off) {
+      if (off == 12) continue;
+      const int32_t nb = row[off];
+      if (nb < 0) continue;
+      if (!(point_box_d2(q.x, q.y, p.bbox[nb]) <= eps_sq)) continue;
+      const int32_t j1 = p.cell_start[nb + 1];
+      for (int32_t j = p.cell_start[nb]; j < j1; ++j) {
+        const float2 pj = p.xy[j];
+        cnt += sq_dist(__fsub_rn(pj.x, q.x), __fsub_rn(pj.y, q.y)) <= eps_sq;
       }
     }
-    bool any_core = false, all_core = true;
-    for (int32_t qb = 0; qb < npts; qb += 32) {
-      const int32_t nq = min(32, npts - qb);
-      float2 q = make_float2(0.f, 0.f);
-      if ((int32_t)lane < nq) q = p.xy[st0 + qb + lane];
-      // Prune mask per query: bit l set when neighbour cell l is not pruned.
-      uint32_t mymask = 0;
-      for (int32_t j = 0; j < nq; ++j) {
-        const float qx = __shfl_sync(kFull, q.x, j), qy = __shfl_sync(kFull, q.y, j);
-        const bool ok = nb >= 0 && point_box_d2(qx, qy, bb) <= eps_sq;
-        const uint32_t m = __ballot_sync(kFull, ok);
-        if ((int32_t)lane == j) mymask = m;
+    p.is_core[i] = cnt >= ms ? 1 : 0;
+  }
+}
+
+// Cell status (dbscan_cuda.cu:250-263) and union-find initialisation
+// (:313-316), one thread per cell.
+__global__ void __launch_bounds__(256) k_status(Plan p) {
+  const uint32_t C = p.desc->num_cells;
+  for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < C; c += gridDim.x * blockDim.x) {
+    const int32_t s0 = p.cell_start[c], s1 = p.cell_start[c + 1];
+    uint8_t st;
+    if (s1 - s0 >= p.seg_param[p.cell_seg[c]].ms) {
+      st = 2;
+    } else {
+      bool any = false, all = true;
+      for (int32_t j = s0; j < s1; ++j) {
+        const bool k = p.is_core[j] != 0;
+        any |= k;
+        all &= k;
       }
-      const uint32_t U = __reduce_or_sync(kFull, (int32_t)lane < nq ? mymask : 0u);
-      const int32_t szU = ((U >> lane) & 1u) ? sz : 0;
-      const int32_t pre = warp_incl_scan(szU);
-      const int32_t T = __shfl_sync(kFull, pre, 31);
-      s_pre[w][lane] = pre;
-      s_off[w][lane] = cs0 - (pre - szU);
-      __syncwarp();
-      int32_t cnt = npts;  // lane j: count of query j
-      for (int32_t f0 = 0; f0 < T; f0 += 32) {
-        const int32_t f = f0 + (int32_t)lane;
-        int l = 0;
-        float2 pj = make_float2(0.f, 0.f);
-        const bool have = f < T;
-        if (have) {
-          l = slice_of(s_pre[w], f);
-          pj = p.xy[f + s_off[w][l]];
-        }
-        for (int32_t j = 0; j < nq; ++j) {
-          const float qx = __shfl_sync(kFull, q.x, j), qy = __shfl_sync(kFull, q.y, j);
-          const uint32_t m = __shfl_sync(kFull, mymask, j);
-          const bool ok = have && ((m >> l) & 1u) &&
-                          sq_dist(__fsub_rn(pj.x, qx), __fsub_rn(pj.y, qy)) <= eps_sq;
-          const uint32_t b = __ballot_sync(kFull, ok);
-          if ((int32_t)lane == j) cnt += __popc(b);
-        }
-        if (__ballot_sync(kFull, (int32_t)lane < nq && cnt < ms) == 0) break;
-      }
-      const bool core = (int32_t)lane < nq && cnt >= ms;
-      if ((int32_t)lane < nq) p.is_core[st0 + qb + lane] = core ? 1 : 0;
-      any_core |= __ballot_sync(kFull, core) != 0;
-      all_core &= __ballot_sync(kFull, (int32_t)lane < nq && !core) == 0;
-      __syncwarp();
+      st = !any ? 0 : (all ? 2 : 1);
     }
-    if (lane == 0) p.cell_status[c] = !any_core ? 0 : (all_core ? 2 : 1);
+    p.cell_status[c] = st;
+    p.uf[c] = (int32_t)c;
   }
 }
 
@@ -218,10 +168,19 @@ __device__ __forceinline__ bool pair_scan(const Plan& p, int32_t c0, int32_t c1,
   return false;
 }
 
-// Ring-1 offsets of the 5x5 stencil (|dx|,|dy| <= 1, centre excluded).
-constexpr uint32_t kRing1 = (1u << 6) | (1u << 7) | (1u << 8) | (1u << 11) | (1u << 13) |
-                            (1u << 16) | (1u << 17) | (1u << 18);
+// Distance tests one lane may spend on its own cell pair before the pair is
+// handed to the whole warp (a dense pair without a close core pair would
+// otherwise cost |c| * |nc| serial tests, the reference's k_unite_pairs
+// worst case).
+constexpr int32_t kPairBudget = 96;
 
+// Edges of the cell graph from core cell c to its neighbours nc > c. Each
+// lane takes one stencil offset and scans its pair serially (i over c's core
+// points passing the point-box prune, j over nc's core points, early exit on
+// the first pair within eps); pairs that exhaust the lane budget are scanned
+// warp-cooperatively afterwards. Found edges are united at once. Whether an
+// edge exists does not depend on the order of the tests, and the components
+// (rooted at their smallest cell) do not depend on the order of the unions.
 __global__ void __launch_bounds__(kCellThreads) k_union(Plan p) {
   const uint32_t lane = lane_id();
   Desc* d = p.desc;
@@ -231,33 +190,46 @@ __global__ void __launch_bounds__(kCellThreads) k_union(Plan p) {
     if (c >= C) break;
     if (p.cell_status[c] == 0) continue;
     const float eps_sq = p.seg_param[p.cell_seg[c]].eps_sq;
+    const float4 bb_c = p.bbox[c];
     int32_t nb = -1;
     bool cand = false;
+    float4 bb_n = make_float4(0.f, 0.f, 0.f, 0.f);
     if (lane < kNgh && lane != 12) {
       nb = p.ngh[(int64_t)c * kNgh + lane];
-      cand = nb > (int32_t)c && p.cell_status[nb] != 0;
-    }
-    const uint32_t mask = __ballot_sync(kFull, cand);
-    if (!mask) continue;
-    const float4 bb_c = p.bbox[c];
-    const int32_t c0 = p.cell_start[c], c1 = p.cell_start[c + 1];
-    // Ring-1 neighbours first: their unions make most ring-2 scans redundant.
-    uint32_t order[2] = {mask & kRing1, mask & ~kRing1};
-    for (int r = 0; r < 2; ++r) {
-      uint32_t m = order[r];
-      while (m) {
-        const int l = __ffs(m) - 1;
-        m &= m - 1;
-        const int32_t nc = __shfl_sync(kFull, nb, l);
-        int same = 0;
-        if (lane == 0) same = uf_find_ro(p.uf, (int32_t)c, d) == uf_find_ro(p.uf, nc, d);
-        if (__shfl_sync(kFull, same, 0)) continue;
-        const float4 bb_n = p.bbox[nc];
-        if (!(box_box_d2(bb_c, bb_n) <= eps_sq)) continue;
-        const bool found = pair_scan(p, c0, c1, p.cell_start[nc], p.cell_start[nc + 1], bb_n, eps_sq);
-        if (found && lane == 0) uf_unite(p.uf, (int32_t)c, nc, d);
-        __syncwarp();
+      if (nb > (int32_t)c && p.cell_status[nb] != 0) {
+        bb_n = p.bbox[nb];
+        cand = box_box_d2(bb_c, bb_n) <= eps_sq;
       }
+    }
+    if (__ballot_sync(kFull, cand) == 0) continue;
+    const int32_t c0 = p.cell_start[c], c1 = p.cell_start[c + 1];
+    bool found = false, deferred = false;
+    if (cand) {
+      const int32_t n0 = p.cell_start[nb], n1 = p.cell_start[nb + 1];
+      int32_t budget = kPairBudget;
+      for (int32_t i = c0; i < c1 && !found && !deferred; ++i) {
+        if (!p.is_core[i]) continue;
+        const float2 pi = p.xy[i];
+        if (!(point_box_d2(pi.x, pi.y, bb_n) <= eps_sq)) continue;
+        for (int32_t j = n0; j < n1; ++j) {
+          if (--budget < 0) { deferred = true; break; }
+          if (!p.is_core[j]) continue;
+          const float2 pj = p.xy[j];
+          if (sq_dist(__fsub_rn(pj.x, pi.x), __fsub_rn(pj.y, pi.y)) <= eps_sq) { found = true; break; }
+        }
+      }
+    }
+    if (found) uf_unite(p.uf, (int32_t)c, nb, d);
+    uint32_t dm = __ballot_sync(kFull, deferred);
+    while (dm) {
+      const int l = __ffs(dm) - 1;
+      dm &= dm - 1;
+      const int32_t nc = __shfl_sync(kFull, nb, l);
+      const float4 bbn = make_float4(__shfl_sync(kFull, bb_n.x, l), __shfl_sync(kFull, bb_n.y, l),
+                                     __shfl_sync(kFull, bb_n.z, l), __shfl_sync(kFull, bb_n.w, l));
+      if (pair_scan(p, c0, c1, p.cell_start[nc], p.cell_start[nc + 1], bbn, eps_sq) && lane == 0)
+        uf_unite(p.uf, (int32_t)c, nc, d);
+      __syncwarp();
     }
   }
 }
@@ -329,134 +301,54 @@ __global__ void __launch_bounds__(kScanThreads) k_ids(Plan p) {
 }
 
 // --------------------------------------------------------------- k_labels
-// Per cell: cluster id of the cell (rank of its root among the cloud's
-// roots), core labels, and for each non-core point the label of the nearest
-// core point within eps, ties to the smaller input index (the (d2, perm[j])
-// rule of dbscan_cuda.cu:447-467), written straight to input order.
-constexpr int kQB = 4;  // queries per pass over the candidates
-
-__device__ __forceinline__ int32_t cluster_of(const Plan& p, int32_t cell, int32_t seg_roots) {
-  return p.cell_status[cell] == 0 ? -1 : p.root_rank[p.uf[cell]] - seg_roots;
-}
-
+// Final label of every sorted point, written straight to input order
+// (k_core_labels :409-417, k_border_assign :427-470, k_unpermute :475-481).
+// A core point takes its cell's cluster id: the rank of the cell's root
+// among the roots of its cloud. A non-core point takes the cluster of the
+// core point within eps that minimises (d2, input index) over the 25 stencil
+// cells with a core point, pruned by the point-box test; -1 when none.
 __global__ void __launch_bounds__(kCellThreads) k_labels(Plan p) {
-  __shared__ int32_t s_pre[kWarpsPerBlock][32];
-  __shared__ int32_t s_off[kWarpsPerBlock][32];
-  __shared__ int32_t s_lab[kWarpsPerBlock][32];
-  const uint32_t lane = lane_id();
-  const uint32_t w = threadIdx.x >> 5;
-  Desc* d = p.desc;
-  const uint32_t C = d->num_cells;
-  while (true) {
-    const uint32_t c = next_cell(&d->ctr[kCtrLabels]);
-    if (c >= C) break;
+  const int64_t n = p.n;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t c = p.point_cell[i];
     const int32_t seg = p.cell_seg[c];
     const int32_t seg_roots = p.root_rank[p.seg_info[seg].cell_begin];
-    const uint8_t st = p.cell_status[c];
-    const int32_t cid = st == 0 ? -1 : p.root_rank[p.uf[c]] - seg_roots;
-    const int32_t st0 = p.cell_start[c], st1 = p.cell_start[c + 1];
-    if (st == 2) {
-      for (int32_t i = st0 + lane; i < st1; i += 32) p.labels[p.perm[i]] = cid;
-      continue;
-    }
-    const float eps_sq = p.seg_param[seg].eps_sq;
-    // Candidate cells: the 25 stencil cells (own cell included) with a core.
-    int32_t nb = -1, sz = 0, cs0 = 0, lab = -1;
-    float4 bb = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (lane < kNgh) {
-      nb = p.ngh[(int64_t)c * kNgh + lane];
-      if (nb >= 0 && p.cell_status[nb] != 0) {
-        cs0 = p.cell_start[nb];
-        sz = p.cell_start[nb + 1] - cs0;
-        bb = p.bbox[nb];
-        lab = cluster_of(p, nb, seg_roots);
-      } else {
-        nb = -1;
+    int32_t lab;
+    if (p.is_core[i]) {
+      lab = p.root_rank[p.uf[c]] - seg_roots;
+    } else {
+      const float eps_sq = p.seg_param[seg].eps_sq;
+      const float2 q = p.xy[i];
+      const int32_t* row = p.ngh + (int64_t)c * kNgh;
+      unsigned long long best = ~0ull;
+      int32_t best_nb = -1;
+      for (int off = 0; off < kNgh; ++off) {
+        const int32_t nb = row[off];
+        if (nb < 0 || p.cell_status[nb] == 0) continue;
+        if (!(point_box_d2(q.x, q.y, p.bbox[nb]) <= eps_sq)) continue;
+        const int32_t j1 = p.cell_start[nb + 1];
+        for (int32_t j = p.cell_start[nb]; j < j1; ++j) {
+          if (!p.is_core[j]) continue;
+          const float2 pj = p.xy[j];
+          const float d2 = sq_dist(__fsub_rn(pj.x, q.x), __fsub_rn(pj.y, q.y));
+          if (d2 <= eps_sq) {
+            // d2 >= +0 and not NaN here, so its bits order like its value.
+            const unsigned long long key = ((unsigned long long)__float_as_uint(d2) << 32) | p.perm[j];
+            if (key < best) { best = key; best_nb = nb; }
+          }
+        }
       }
+      lab = best_nb < 0 ? -1 : p.root_rank[p.uf[best_nb]] - seg_roots;
     }
-    s_lab[w][lane] = lab;
-    for (int32_t ib = st0; ib < st1; ib += 32) {
-      const int32_t i = ib + (int32_t)lane;
-      const bool in = i < st1;
-      const bool core = in && p.is_core[i];
-      int32_t pi = 0;
-      float2 q = make_float2(0.f, 0.f);
-      if (in) { pi = (int32_t)p.perm[i]; q = p.xy[i]; }
-      if (core) p.labels[pi] = cid;
-      uint32_t qmask = __ballot_sync(kFull, in && !core);
-      while (qmask) {
-        // Up to kQB queries this pass.
-        int ql[kQB];
-        uint32_t mk[kQB];
-        float qx[kQB], qy[kQB];
-        uint32_t U = 0;
-#pragma unroll
-        for (int t = 0; t < kQB; ++t) {
-          ql[t] = qmask ? __ffs(qmask) - 1 : -1;
-          if (qmask) qmask &= qmask - 1;
-          mk[t] = 0;
-          qx[t] = 0.f; qy[t] = 0.f;
-          if (ql[t] >= 0) {
-            qx[t] = __shfl_sync(kFull, q.x, ql[t]);
-            qy[t] = __shfl_sync(kFull, q.y, ql[t]);
-            mk[t] = __ballot_sync(kFull, nb >= 0 && point_box_d2(qx[t], qy[t], bb) <= eps_sq);
-            U |= mk[t];
-          }
-        }
-        const int32_t szU = ((U >> lane) & 1u) ? sz : 0;
-        const int32_t pre = warp_incl_scan(szU);
-        const int32_t T = __shfl_sync(kFull, pre, 31);
-        s_pre[w][lane] = pre;
-        s_off[w][lane] = cs0 - (pre - szU);
-        __syncwarp();
-        unsigned long long best[kQB];
-        int32_t blab[kQB];
-#pragma unroll
-        for (int t = 0; t < kQB; ++t) { best[t] = ~0ull; blab[t] = -1; }
-        for (int32_t f0 = 0; f0 < T; f0 += 32) {
-          const int32_t f = f0 + (int32_t)lane;
-          if (f < T) {
-            const int l = slice_of(s_pre[w], f);
-            const int32_t j = f + s_off[w][l];
-            if (p.is_core[j]) {
-              const float2 pj = p.xy[j];
-              const uint32_t pm = p.perm[j];
-              const int32_t lj = s_lab[w][l];
-#pragma unroll
-              for (int t = 0; t < kQB; ++t) {
-                if ((mk[t] >> l) & 1u) {
-                  const float d2 = sq_dist(__fsub_rn(pj.x, qx[t]), __fsub_rn(pj.y, qy[t]));
-                  if (d2 <= eps_sq) {
-                    const unsigned long long key =
-                        ((unsigned long long)__float_as_uint(d2) << 32) | pm;
-                    if (key < best[t]) { best[t] = key; blab[t] = lj; }
-                  }
-                }
-              }
-            }
-          }
-        }
-#pragma unroll
-        for (int t = 0; t < kQB; ++t) {
-          unsigned long long b = best[t];
-          int32_t bl = blab[t];
-#pragma unroll
-          for (int o = 16; o > 0; o >>= 1) {
-            const unsigned long long ob = __shfl_xor_sync(kFull, b, o);
-            const int32_t ol = __shfl_xor_sync(kFull, bl, o);
-            if (ob < b) { b = ob; bl = ol; }
-          }
-          if (ql[t] >= 0 && (int)lane == ql[t]) p.labels[pi] = bl;
-        }
-        __syncwarp();
-      }
-    }
+    p.labels[p.perm[i]] = lab;
   }
 }
 
 // ------------------------------------------------------------- launchers
 cudaError_t launch_core(const Plan& p, cudaStream_t s) {
   k_core<<<p.num_sms * 8, kCellThreads, 0, s>>>(p);
+  k_status<<<p.num_sms * 8, 256, 0, s>>>(p);
   return cudaGetLastError();
 }
 

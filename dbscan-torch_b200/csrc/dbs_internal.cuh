@@ -83,6 +83,9 @@ struct SegParam {
 // non-negative and negative classes so that the compaction preserves the
 // reference's unsigned key order ((u32)kx << 32 | (u32)ky): non-negative
 // coordinates come first, then negative ones, each class ascending.
+// The compacted key of cell (gx, gy) is base + (gx << ysh) + gy with
+// ysh = ceil(log2(wy)): lexicographic in (gx, gy), and a cell's coordinates
+// come back from its key with a shift and a mask.
 struct SegInfo {
   int32_t bx[4];     // x: lo_pos, hi_pos, lo_neg, hi_neg (atomics)
   int32_t by[4];     // y: same
@@ -91,7 +94,7 @@ struct SegInfo {
   uint64_t base;     // first global key of this cloud
   int64_t map_base;  // offset in the dense cell map, -1 when not dense
   int32_t cell_begin;  // first cell index of this cloud (filled by k_rle)
-  int32_t pad;
+  uint32_t ysh;      // bits of the y part of the local key
 };
 
 struct Desc {
@@ -122,6 +125,7 @@ struct Plan {
   unsigned long long* sweep_status[2];  // onesweep look-back words
   unsigned long long* rle_status;
   unsigned long long* ids_status;
+  int32_t* point_cell;    // (n) cell of each sorted point
   int32_t* cell_start;    // (n+1)
   uint64_t* cell_key;     // (n)
   int32_t* cell_seg;      // (n)
