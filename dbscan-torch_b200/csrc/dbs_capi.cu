@@ -38,7 +38,6 @@ size_t carve(int64_t n, int32_t nseg, char* base, Plan* p) {
   std::memset(&q, 0, sizeof(q));
   Carver cv{base};
   const size_t N = (size_t)(n > 0 ? n : 1);
-  const int32_t sweep_tiles = (int32_t)((N + kSortTile - 1) / kSortTile);
   const int32_t scan_tiles = (int32_t)((N + kScanTile - 1) / kScanTile);
   q.desc = cv.take<Desc>(1);
   q.seg_off = cv.take<int64_t>((size_t)nseg + 1);
@@ -51,8 +50,7 @@ size_t carve(int64_t n, int32_t nseg, char* base, Plan* p) {
   q.perm = cv.take<uint32_t>(N);
   q.xy = cv.take<float2>(N);
   q.is_core = cv.take<uint8_t>(N);
-  q.sweep_status[0] = cv.take<unsigned long long>((size_t)sweep_tiles * kRadix);
-  q.sweep_status[1] = cv.take<unsigned long long>((size_t)sweep_tiles * kRadix);
+  q.chunk_count = cv.take<uint32_t>((size_t)kRadix * kMaxChunks);
   q.rle_status = cv.take<unsigned long long>((size_t)scan_tiles);
   q.ids_status = cv.take<unsigned long long>((size_t)scan_tiles);
   q.point_cell = cv.take<int32_t>(N);
@@ -66,12 +64,31 @@ size_t carve(int64_t n, int32_t nseg, char* base, Plan* p) {
   q.root_rank = cv.take<int32_t>(N);
   q.dense_cap = kDenseFactor * (int64_t)N + kDenseSlack * (int64_t)nseg;
   q.cell_map = cv.take<int32_t>((size_t)q.dense_cap);
+  q.big_cap = (int64_t)(N / kHugeCell) + 1;
+  q.chunk_cap = (int64_t)(N / kHugeChunk) + q.big_cap + 1;
+  q.big_cell = cv.take<int32_t>((size_t)q.big_cap);
+  q.big_base = cv.take<unsigned long long>((size_t)q.big_cap);
+  q.big_done = cv.take<uint32_t>((size_t)q.big_cap);
+  q.big_chunk_box = cv.take<float4>((size_t)q.chunk_cap);
   q.n = n;
   q.nseg = nseg;
-  q.sweep_tiles = sweep_tiles;
   q.scan_tiles = scan_tiles;
   if (p) *p = q;
   return cv.off;
+}
+
+// Radix-pass chunks: about three resident scatter blocks per SM, each
+// owning a whole number of kSortTile tiles.
+void set_chunking(Plan* p) {
+  const int64_t tiles = (p->n + kSortTile - 1) / kSortTile;
+  int64_t target = (int64_t)p->num_sms * 3;
+  if (target > kMaxChunks) target = kMaxChunks;
+  if (target < 1) target = 1;
+  int64_t per = (tiles + target - 1) / target;
+  if (per < 1) per = 1;
+  p->chunk_tiles = (int32_t)per;
+  p->sort_chunks = (int32_t)((tiles + per - 1) / per);
+  if (p->sort_chunks < 1) p->sort_chunks = 1;
 }
 
 int num_sms_current() {
@@ -151,6 +168,7 @@ int prepare_single(const float* X, int64_t n, double eps, int64_t min_samples, i
   p->X = reinterpret_cast<const float2*>(X);
   p->labels = labels;
   p->num_sms = num_sms_current();
+  set_chunking(p);
   p->single = 1;
   p->single_param = make_param(eps, min_samples);
   return DBS_OK;
@@ -307,6 +325,7 @@ int dbs_dbscan2d_batched_device(const float* X, int64_t n_total, int32_t nseg,
   p.X = reinterpret_cast<const float2*>(X);
   p.labels = labels;
   p.num_sms = num_sms_current();
+  set_chunking(&p);
   p.single = 0;
   return run_pipeline(p, s, nullptr);
 }
@@ -343,6 +362,7 @@ int dbs_dbscan2d_batched(const float* X, const int64_t* seg_offsets, const doubl
   p.X = reinterpret_cast<const float2*>(X);
   p.labels = labels;
   p.num_sms = num_sms_current();
+  set_chunking(&p);
   p.single = 0;
   return run_pipeline(p, s, nullptr);
 }

@@ -168,7 +168,19 @@ __global__ void __launch_bounds__(kCellThreads) k_cell_prep(Plan p) {
       }
       p.bbox[c] = b;
     }
-    uint32_t bm = __ballot_sync(full, big);
+    const bool huge = big && (s1 - s0) > kHugeCell;
+    if (huge) {
+      // Registered for k_huge_bbox: one entry, ceil(size / kHugeChunk) chunks.
+      const unsigned long long nch = (unsigned long long)((s1 - s0 + kHugeChunk - 1) / kHugeChunk);
+      const unsigned long long old = atomicAdd(&p.desc->big_packed, (1ull << 40) + nch);
+      const unsigned long long e = old >> 40;
+      if ((int64_t)e < p.big_cap) {
+        p.big_cell[e] = (int32_t)c;
+        p.big_base[e] = old & ((1ull << 40) - 1);
+        p.big_done[e] = 0;
+      }
+    }
+    uint32_t bm = __ballot_sync(full, big && !huge);
     while (bm) {
       const int l = __ffs(bm) - 1;
       bm &= bm - 1;
@@ -215,6 +227,75 @@ __global__ void __launch_bounds__(kCellThreads) k_cell_prep(Plan p) {
   }
 }
 
+// Bounding boxes of huge cells (more than kHugeCell points, e.g. a 2M-point
+// dense square): every warp of the grid takes kHugeChunk-point chunks of
+// any huge cell, reduces the chunk, and the warp that finishes a cell's last
+// chunk folds the cell's chunk boxes into bbox[c]. Min and max are
+// order-independent, so the box equals the reference's serial fold.
+__global__ void __launch_bounds__(256) k_huge_bbox(Plan p) {
+  const uint32_t full = 0xffffffffu;
+  const uint32_t lane = lane_id();
+  Desc* d = p.desc;
+  const unsigned long long packed = d->big_packed;
+  const int64_t entries = min((int64_t)(packed >> 40), p.big_cap);
+  const int64_t chunks = min((int64_t)(packed & ((1ull << 40) - 1)), p.chunk_cap);
+  if (entries == 0) return;
+  while (true) {
+    uint32_t g = 0;
+    if (lane == 0) g = atomicAdd(&d->ctr[kCtrBig], 1u);
+    g = __shfl_sync(full, g, 0);
+    if ((int64_t)g >= chunks) break;
+    // Entry owning chunk g: last entry with big_base <= g.
+    int64_t lo = 0, hi = entries - 1;
+    while (lo < hi) {
+      const int64_t mid = (lo + hi + 1) >> 1;
+      if (p.big_base[mid] <= g) lo = mid; else hi = mid - 1;
+    }
+    const int32_t c = p.big_cell[lo];
+    const int32_t s0 = p.cell_start[c], s1 = p.cell_start[c + 1];
+    const int32_t k = (int32_t)(g - p.big_base[lo]);
+    const int32_t a = s0 + k * kHugeChunk, b = min(s1, a + kHugeChunk);
+    float xmin = INFINITY, xmax = -INFINITY, ymin = INFINITY, ymax = -INFINITY;
+    for (int32_t i = a + lane; i < b; i += 32) {
+      const float2 v = p.xy[i];
+      xmin = fminf(xmin, v.x); xmax = fmaxf(xmax, v.x);
+      ymin = fminf(ymin, v.y); ymax = fmaxf(ymax, v.y);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      xmin = fminf(xmin, __shfl_xor_sync(full, xmin, o));
+      xmax = fmaxf(xmax, __shfl_xor_sync(full, xmax, o));
+      ymin = fminf(ymin, __shfl_xor_sync(full, ymin, o));
+      ymax = fmaxf(ymax, __shfl_xor_sync(full, ymax, o));
+    }
+    const int32_t nch = (s1 - s0 + kHugeChunk - 1) / kHugeChunk;
+    uint32_t last = 0;
+    if (lane == 0) {
+      p.big_chunk_box[g] = make_float4(xmin, xmax, ymin, ymax);
+      __threadfence();
+      last = atomicAdd(&p.big_done[lo], 1u) == (uint32_t)(nch - 1);
+    }
+    if (__shfl_sync(full, last, 0)) {
+      __threadfence();
+      const int64_t b0 = (int64_t)p.big_base[lo];
+      xmin = INFINITY; xmax = -INFINITY; ymin = INFINITY; ymax = -INFINITY;
+      for (int32_t t = lane; t < nch; t += 32) {
+        const float4 v = __ldcg(&p.big_chunk_box[b0 + t]);
+        xmin = fminf(xmin, v.x); xmax = fmaxf(xmax, v.y);
+        ymin = fminf(ymin, v.z); ymax = fmaxf(ymax, v.w);
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        xmin = fminf(xmin, __shfl_xor_sync(full, xmin, o));
+        xmax = fmaxf(xmax, __shfl_xor_sync(full, xmax, o));
+        ymin = fminf(ymin, __shfl_xor_sync(full, ymin, o));
+        ymax = fmaxf(ymax, __shfl_xor_sync(full, ymax, o));
+      }
+      if (lane == 0) p.bbox[c] = make_float4(xmin, xmax, ymin, ymax);
+    }
+  }
+}
+
 // ------------------------------------------------------------- launchers
 cudaError_t launch_rle(const Plan& p, cudaStream_t s) {
   int grid = p.num_sms * 4;
@@ -225,6 +306,7 @@ cudaError_t launch_rle(const Plan& p, cudaStream_t s) {
 
 cudaError_t launch_cell_prep(const Plan& p, cudaStream_t s) {
   k_cell_prep<<<p.num_sms * 4, kCellThreads, 0, s>>>(p);
+  k_huge_bbox<<<p.num_sms * 4, 256, 0, s>>>(p);
   return cudaGetLastError();
 }
 

@@ -19,11 +19,6 @@ namespace dbs {
 
 constexpr uint32_t kFull = 0xffffffffu;
 
-__device__ __forceinline__ uint32_t next_cell(uint32_t* ctr) {
-  uint32_t c = 0;
-  if (lane_id() == 0) c = atomicAdd(ctr, 1u);
-  return __shfl_sync(kFull, c, 0);
-}
 
 // ----------------------------------------------------------------- k_core
 // Core flag of every sorted point, one thread per point. A point of a cell
@@ -126,16 +121,20 @@ __device__ __forceinline__ void uf_unite(int32_t* uf, int32_t a, int32_t b, Desc
 
 // Is there a core point i of cell c and a core point j of cell nc with
 // point_box_d2(i, bbox[nc]) <= eps_sq and d2(i, j) <= eps_sq? (the pair scan
-// of dbscan_cuda.cu:353-368, warp-cooperative).
+// of dbscan_cuda.cu:353-368, warp-cooperative). Points j farther than eps
+// from c's box are skipped as well: with the monotone distance form every
+// pair they belong to is farther than eps, so the answer is unchanged.
 __device__ __forceinline__ bool pair_scan(const Plan& p, int32_t c0, int32_t c1, int32_t n0,
-                                          int32_t n1, float4 bb_n, float eps_sq) {
+                                          int32_t n1, float4 bb_c, float4 bb_n, float eps_sq) {
   const uint32_t lane = lane_id();
   // First chunk of nc cached in registers.
   const int32_t j = n0 + (int32_t)lane;
-  const bool jin = j < n1;
-  const bool jcore = jin && p.is_core[j];
+  bool jok = j < n1 && p.is_core[j];
   float2 pjr = make_float2(0.f, 0.f);
-  if (jcore) pjr = p.xy[j];
+  if (jok) {
+    pjr = p.xy[j];
+    jok = point_box_d2(pjr.x, pjr.y, bb_c) <= eps_sq;
+  }
   const bool one_chunk = (n1 - n0) <= 32;
   for (int32_t ib = c0; ib < c1; ib += 32) {
     const int32_t i = ib + (int32_t)lane;
@@ -150,7 +149,7 @@ __device__ __forceinline__ bool pair_scan(const Plan& p, int32_t c0, int32_t c1,
       const int q = __ffs(cm) - 1;
       cm &= cm - 1;
       const float qx = __shfl_sync(kFull, pi.x, q), qy = __shfl_sync(kFull, pi.y, q);
-      bool hit = jcore && sq_dist(__fsub_rn(pjr.x, qx), __fsub_rn(pjr.y, qy)) <= eps_sq;
+      bool hit = jok && sq_dist(__fsub_rn(pjr.x, qx), __fsub_rn(pjr.y, qy)) <= eps_sq;
       if (__any_sync(kFull, hit)) return true;
       if (!one_chunk) {
         for (int32_t jb = n0 + 32; jb < n1; jb += 32) {
@@ -158,7 +157,8 @@ __device__ __forceinline__ bool pair_scan(const Plan& p, int32_t c0, int32_t c1,
           bool h = false;
           if (jj < n1 && p.is_core[jj]) {
             const float2 pj = p.xy[jj];
-            h = sq_dist(__fsub_rn(pj.x, qx), __fsub_rn(pj.y, qy)) <= eps_sq;
+            h = point_box_d2(pj.x, pj.y, bb_c) <= eps_sq &&
+                sq_dist(__fsub_rn(pj.x, qx), __fsub_rn(pj.y, qy)) <= eps_sq;
           }
           if (__any_sync(kFull, h)) return true;
         }
@@ -174,37 +174,56 @@ __device__ __forceinline__ bool pair_scan(const Plan& p, int32_t c0, int32_t c1,
 // worst case).
 constexpr int32_t kPairBudget = 96;
 
-// Edges of the cell graph from core cell c to its neighbours nc > c. Each
-// lane takes one stencil offset and scans its pair serially (i over c's core
-// points passing the point-box prune, j over nc's core points, early exit on
-// the first pair within eps); pairs that exhaust the lane budget are scanned
-// warp-cooperatively afterwards. Found edges are united at once. Whether an
-// edge exists does not depend on the order of the tests, and the components
-// (rooted at their smallest cell) do not depend on the order of the unions.
-__global__ void __launch_bounds__(kCellThreads) k_union(Plan p) {
+// Stencil offsets (off = (dx+2)*5 + (dy+2)) of ring 1 (|dx|, |dy| <= 1) and
+// ring 2, centre excluded.
+__constant__ int8_t kRingOffs[2][16] = {
+    {6, 7, 8, 11, 13, 16, 17, 18, 0, 0, 0, 0, 0, 0, 0, 0},
+    {0, 1, 2, 3, 4, 5, 9, 10, 14, 15, 19, 20, 21, 22, 23, 24}};
+
+// Edges of the cell graph from core cell c to its neighbours nc > c at the
+// offsets of one ring, one thread per (cell, offset). A thread scans its
+// pair serially (i over c's core points passing the point-box prune against
+// nc, j over nc's core points, early exit on the first pair within eps);
+// pairs that exhaust the thread's budget are scanned by the whole warp
+// afterwards (pair_scan). Found edges are united at once. With
+// `skip_united`, a pair already in one component (read-only finds) is not
+// scanned. Whether an edge exists does not depend on the order of the tests,
+// and the components (rooted at their smallest cell) do not depend on the
+// order of the unions, so running ring 1 first and ring 2 after a flatten
+// (when most dense cells are already connected) changes only the work.
+__global__ void __launch_bounds__(kCellThreads) k_union(Plan p, int ring, int skip_united) {
   const uint32_t lane = lane_id();
   Desc* d = p.desc;
   const uint32_t C = d->num_cells;
-  while (true) {
-    const uint32_t c = next_cell(&d->ctr[kCtrUnion]);
-    if (c >= C) break;
-    if (p.cell_status[c] == 0) continue;
-    const float eps_sq = p.seg_param[p.cell_seg[c]].eps_sq;
-    const float4 bb_c = p.bbox[c];
-    int32_t nb = -1;
+  const int nofs = ring == 0 ? 8 : 16;
+  const int64_t total = (int64_t)C * nofs;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t base = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; base < total;
+       base += nwarps * 32) {
+    const int64_t t = base + lane;
+    int32_t c = 0, nb = -1;
     bool cand = false;
-    float4 bb_n = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (lane < kNgh && lane != 12) {
-      nb = p.ngh[(int64_t)c * kNgh + lane];
-      if (nb > (int32_t)c && p.cell_status[nb] != 0) {
-        bb_n = p.bbox[nb];
-        cand = box_box_d2(bb_c, bb_n) <= eps_sq;
+    float eps_sq = 0.f;
+    float4 bb_c = make_float4(0.f, 0.f, 0.f, 0.f), bb_n = bb_c;
+    if (t < total) {
+      c = (int32_t)(t / nofs);
+      const int off = kRingOffs[ring][t - (int64_t)c * nofs];
+      if (p.cell_status[c] != 0) {
+        nb = p.ngh[(int64_t)c * kNgh + off];
+        if (nb > c && p.cell_status[nb] != 0) {
+          eps_sq = p.seg_param[p.cell_seg[c]].eps_sq;
+          bb_c = p.bbox[c];
+          bb_n = p.bbox[nb];
+          cand = box_box_d2(bb_c, bb_n) <= eps_sq;
+          if (cand && skip_united) cand = uf_find_ro(p.uf, c, d) != uf_find_ro(p.uf, nb, d);
+        }
       }
     }
-    if (__ballot_sync(kFull, cand) == 0) continue;
-    const int32_t c0 = p.cell_start[c], c1 = p.cell_start[c + 1];
     bool found = false, deferred = false;
+    int32_t c0 = 0, c1 = 0;
     if (cand) {
+      c0 = p.cell_start[c];
+      c1 = p.cell_start[c + 1];
       const int32_t n0 = p.cell_start[nb], n1 = p.cell_start[nb + 1];
       int32_t budget = kPairBudget;
       for (int32_t i = c0; i < c1 && !found && !deferred; ++i) {
@@ -219,19 +238,34 @@ __global__ void __launch_bounds__(kCellThreads) k_union(Plan p) {
         }
       }
     }
-    if (found) uf_unite(p.uf, (int32_t)c, nb, d);
+    if (found) uf_unite(p.uf, c, nb, d);
     uint32_t dm = __ballot_sync(kFull, deferred);
     while (dm) {
       const int l = __ffs(dm) - 1;
       dm &= dm - 1;
+      const int32_t cc = __shfl_sync(kFull, c, l);
       const int32_t nc = __shfl_sync(kFull, nb, l);
+      const float e2 = __shfl_sync(kFull, eps_sq, l);
+      const float4 bbc = make_float4(__shfl_sync(kFull, bb_c.x, l), __shfl_sync(kFull, bb_c.y, l),
+                                     __shfl_sync(kFull, bb_c.z, l), __shfl_sync(kFull, bb_c.w, l));
       const float4 bbn = make_float4(__shfl_sync(kFull, bb_n.x, l), __shfl_sync(kFull, bb_n.y, l),
                                      __shfl_sync(kFull, bb_n.z, l), __shfl_sync(kFull, bb_n.w, l));
-      if (pair_scan(p, c0, c1, p.cell_start[nc], p.cell_start[nc + 1], bbn, eps_sq) && lane == 0)
-        uf_unite(p.uf, (int32_t)c, nc, d);
+      const int32_t a0 = __shfl_sync(kFull, c0, l), a1 = __shfl_sync(kFull, c1, l);
+      if (pair_scan(p, a0, a1, p.cell_start[nc], p.cell_start[nc + 1], bbc, bbn, e2) && lane == 0)
+        uf_unite(p.uf, cc, nc, d);
       __syncwarp();
     }
   }
+}
+
+// Point every cell at its current root (read-only walks: a concurrent
+// writer of uf[c] only ever stores an ancestor of c, so walks still end at
+// the root).
+__global__ void __launch_bounds__(256) k_flatten(Plan p) {
+  Desc* d = p.desc;
+  const uint32_t C = d->num_cells;
+  for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < C; c += gridDim.x * blockDim.x)
+    p.uf[c] = uf_find_ro(p.uf, (int32_t)c, d);
 }
 
 // ------------------------------------------------------------------ k_ids
@@ -353,7 +387,9 @@ cudaError_t launch_core(const Plan& p, cudaStream_t s) {
 }
 
 cudaError_t launch_union(const Plan& p, cudaStream_t s) {
-  k_union<<<p.num_sms * 8, kCellThreads, 0, s>>>(p);
+  k_union<<<p.num_sms * 8, kCellThreads, 0, s>>>(p, 0, 0);
+  k_flatten<<<p.num_sms * 8, 256, 0, s>>>(p);
+  k_union<<<p.num_sms * 8, kCellThreads, 0, s>>>(p, 1, 1);
   return cudaGetLastError();
 }
 

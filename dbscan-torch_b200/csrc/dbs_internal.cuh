@@ -8,8 +8,8 @@
 //   k_init         zero per-call counters, histograms, per-cloud bounds
 //   k_bounds       per-cloud bounds of the cell coordinates (kx, ky)
 //   k_seg_finalize per-cloud compacted key ranges, key bases, pass count
-//   k_keys_hist    compacted cell keys + every radix digit's histogram
-//   k_onesweep x8  LSD radix passes with decoupled look-back; passes past the
+//   k_keys         compacted cell keys + first-digit histogram per chunk
+//   k_sort_* x8    LSD radix passes (count, scan, scatter); passes past the
 //                  device-side pass count return at once; the last real pass
 //                  also gathers the sorted float2 coordinates and perm
 //   k_rle          run-length cells: cell_start, cell_key, cell map
@@ -36,6 +36,7 @@ constexpr int kSortThreads = 256;
 constexpr int kSortWarps = kSortThreads / 32;
 constexpr int kSortItems = 16;
 constexpr int kSortTile = kSortThreads * kSortItems;
+constexpr int kMaxChunks = 1024;
 constexpr int kScanThreads = 256;
 constexpr int kScanItems = 16;
 constexpr int kScanTile = kScanThreads * kScanItems;
@@ -43,6 +44,8 @@ constexpr int kCellThreads = 256;               // warp-per-cell kernels
 constexpr uint32_t kSpinCap = 1u << 22;         // bounded waits (look-back polls)
 constexpr uint32_t kFindCap = 1u << 20;         // bounded union-find walks / retries
 constexpr int kNgh = 25;
+constexpr int32_t kHugeCell = 4096;   // cells whose box is reduced by many warps
+constexpr int32_t kHugeChunk = 2048;  // points per chunk of a huge cell
 
 // Dense cell map: a cloud whose compacted key range W satisfies
 // W <= kDenseFactor * N + kDenseSlack resolves neighbours with one load.
@@ -58,13 +61,12 @@ enum : uint32_t {
 
 // Dynamic work counters (Desc::ctr).
 enum : int {
-  kCtrPass0 = 0,            // kMaxPasses counters, one per onesweep pass
-  kCtrRle = kMaxPasses,
+  kCtrRle = 0,
   kCtrPrep,
   kCtrCore,
-  kCtrUnion,
   kCtrIds,
   kCtrLabels,
+  kCtrBig,
   kCtrDebug,
   kNumCtr
 };
@@ -105,8 +107,9 @@ struct Desc {
   uint32_t num_cells;
   uint32_t pad0;
   uint64_t dense_total;  // dense-map entries in use
+  unsigned long long big_packed;  // huge cells: entries << 40 | chunks
   uint32_t ctr[kNumCtr];
-  uint32_t hist[kMaxPasses][kRadix];
+  uint32_t digit_total[2][kRadix];  // per-pass digit totals (ping-pong)
 };
 
 // Device pointers of one call, carved out of the caller's workspace.
@@ -122,7 +125,7 @@ struct Plan {
   uint32_t* perm;         // (n) sorted position -> input index
   float2* xy;             // (n) sorted coordinates
   uint8_t* is_core;       // (n) sorted order
-  unsigned long long* sweep_status[2];  // onesweep look-back words
+  uint32_t* chunk_count;  // (kRadix * sort_chunks) digit-major counts / offsets
   unsigned long long* rle_status;
   unsigned long long* ids_status;
   int32_t* point_cell;    // (n) cell of each sorted point
@@ -136,9 +139,16 @@ struct Plan {
   int32_t* root_rank;     // (n) exclusive scan of root flags
   int32_t* cell_map;      // dense cell map
   int64_t dense_cap;      // entries available in cell_map
+  int32_t* big_cell;      // huge cells (> kHugeCell points): cell index
+  unsigned long long* big_base;  // first chunk of each huge cell
+  uint32_t* big_done;     // chunks finished per huge cell
+  float4* big_chunk_box;  // bounding box of each chunk
+  int64_t big_cap;        // entries available in big_cell
+  int64_t chunk_cap;      // entries available in big_chunk_box
   int64_t n;
   int32_t nseg;
-  int32_t sweep_tiles;    // ceil(n / kSortTile)
+  int32_t sort_chunks;    // chunks of the radix passes (one block each)
+  int32_t chunk_tiles;    // kSortTile tiles per chunk
   int32_t scan_tiles;     // ceil(n / kScanTile)
   int32_t num_sms;
   int32_t single;         // one cloud: k_init writes seg_off / seg_param
@@ -230,30 +240,42 @@ constexpr unsigned long long kFlagInc = 2ull << 62;
 constexpr unsigned long long kValMask = (1ull << 62) - 1;
 
 // Decoupled look-back over look-back words laid out with `stride` between
-// consecutive tiles. Returns the exclusive prefix of tile `tile`. Bounded:
-// a wait that exceeds kSpinCap polls sets kErrLookback and gives up.
+// consecutive tiles. Returns the exclusive prefix of tile `tile`. Each poll
+// reads a window of kLookWindow predecessors with independent loads, so a
+// walk over many published aggregates costs one round trip per window.
+// Bounded: a wait that exceeds kSpinCap polls sets kErrLookback and gives up.
+constexpr int kLookWindow = 8;
+
 __device__ __forceinline__ unsigned long long lookback(const unsigned long long* words,
                                                        int64_t tile, int64_t stride, Desc* d) {
   unsigned long long excl = 0;
   int64_t j = tile - 1;
   uint32_t spins = 0;
   while (j >= 0) {
-    unsigned long long v = ld_relaxed(words + j * stride);
-    unsigned long long flag = v & ~kValMask;
-    if (flag == 0) {
-      if (++spins > kSpinCap) { set_error(d, kErrLookback); break; }
-      continue;
+    unsigned long long v[kLookWindow];
+#pragma unroll
+    for (int k = 0; k < kLookWindow; ++k)
+      v[k] = (j - k >= 0) ? ld_relaxed(words + (j - k) * stride) : kFlagInc;
+    int k = 0;
+#pragma unroll
+    for (; k < kLookWindow; ++k) {
+      const unsigned long long flag = v[k] & ~kValMask;
+      if (flag == 0) break;
+      excl += v[k] & kValMask;
+      if (flag == kFlagInc) return excl;
     }
-    excl += v & kValMask;
-    if (flag == kFlagInc) break;
-    --j;
+    j -= k;
+    if (k < kLookWindow && ++spins > kSpinCap) {
+      set_error(d, kErrLookback);
+      break;
+    }
   }
   return excl;
 }
 
 // --------------------------------------------------------- host launchers
 // Each returns cudaGetLastError() of its launches.
-cudaError_t launch_front(const Plan& p, cudaStream_t s);      // init, bounds, finalize, keys_hist
+cudaError_t launch_front(const Plan& p, cudaStream_t s);      // init, bounds, finalize, keys
 cudaError_t launch_sort_pass(const Plan& p, int pass, cudaStream_t s);
 cudaError_t launch_rle(const Plan& p, cudaStream_t s);
 cudaError_t launch_cell_prep(const Plan& p, cudaStream_t s);

@@ -38,14 +38,15 @@ __global__ void k_init(Plan p) {
     d->npasses = 1;
     d->num_cells = 0;
     d->dense_total = 0;
+    d->big_packed = 0;
   }
+  for (int64_t i = tid; i < 2 * kRadix; i += stride) (&d->digit_total[0][0])[i] = 0;
   if (p.single && tid == 0) {
     p.seg_off[0] = 0;
     p.seg_off[1] = p.n;
     p.seg_param[0] = p.single_param;
   }
   for (int64_t i = tid; i < kNumCtr; i += stride) d->ctr[i] = 0;
-  for (int64_t i = tid; i < kMaxPasses * kRadix; i += stride) (&d->hist[0][0])[i] = 0;
   for (int64_t s = tid; s < p.nseg; s += stride) {
     SegInfo& g = p.seg_info[s];
     g.bx[0] = INT32_MAX; g.bx[1] = -1; g.bx[2] = 0; g.bx[3] = INT32_MIN;
@@ -233,14 +234,16 @@ __global__ void __launch_bounds__(1024) k_seg_finalize(Plan p) {
   }
 }
 
-// ------------------------------------------------------------ k_keys_hist
+// ---------------------------------------------------------------- k_keys
+// Compacted cell keys, one block per sort chunk, plus the chunk's histogram
+// of the first digit (the count step of pass 0).
 template <typename K>
-__device__ __forceinline__ void keys_hist_body(const Plan& p, uint32_t (*sh)[kRadix], uint32_t npasses) {
+__device__ __forceinline__ void keys_body(const Plan& p, uint32_t (*h)[kRadix]) {
   const int64_t n = p.n;
   K* keys = reinterpret_cast<K*>(p.keys[0]);
-  const int64_t per_block = (n + gridDim.x - 1) / gridDim.x;
-  const int64_t b0 = (int64_t)blockIdx.x * per_block;
-  const int64_t b1 = min(n, b0 + per_block);
+  const int64_t b0 = (int64_t)blockIdx.x * p.chunk_tiles * kSortTile;
+  const int64_t b1 = min(n, b0 + (int64_t)p.chunk_tiles * kSortTile);
+  const uint32_t warp = threadIdx.x >> 5;
   int32_t seg = b0 < b1 ? seg_of(p, b0) : 0;
   for (int64_t i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
     while (i >= p.seg_off[seg + 1]) ++seg;
@@ -251,48 +254,139 @@ __device__ __forceinline__ void keys_hist_body(const Plan& p, uint32_t (*sh)[kRa
     const uint64_t gy = compact_axis(cell_coord(v.y, inv_r), g.by, g.py);
     const uint64_t key = g.base + (gx << g.ysh) + gy;
     keys[i] = (K)key;
-    for (uint32_t ps = 0; ps < npasses; ++ps)
-      atomicAdd(&sh[ps][(key >> (ps * kRadixBits)) & (kRadix - 1)], 1u);
+    atomicAdd(&h[warp][key & (kRadix - 1)], 1u);
   }
 }
 
-__global__ void __launch_bounds__(256) k_keys_hist(Plan p) {
-  __shared__ uint32_t sh[kMaxPasses][kRadix];
+__global__ void __launch_bounds__(kSortThreads) k_keys(Plan p) {
+  __shared__ uint32_t h[kSortWarps][kRadix];
   Desc* d = p.desc;
-  const uint32_t npasses = d->npasses;
-  for (int i = threadIdx.x; i < kMaxPasses * kRadix; i += blockDim.x) (&sh[0][0])[i] = 0;
+  for (int i = threadIdx.x; i < kSortWarps * kRadix; i += blockDim.x) (&h[0][0])[i] = 0;
   __syncthreads();
-  if (d->key64) keys_hist_body<uint64_t>(p, sh, npasses);
-  else keys_hist_body<uint32_t>(p, sh, npasses);
+  if (d->key64) keys_body<uint64_t>(p, h);
+  else keys_body<uint32_t>(p, h);
   __syncthreads();
-  for (int i = threadIdx.x; i < (int)npasses * kRadix; i += blockDim.x) {
-    const uint32_t v = (&sh[0][0])[i];
-    if (v) atomicAdd(&(&d->hist[0][0])[i], v);
+  {
+    const uint32_t t = threadIdx.x;
+    uint32_t sum = 0;
+#pragma unroll
+    for (int w = 0; w < kSortWarps; ++w) sum += h[w][t];
+    p.chunk_count[(int64_t)t * p.sort_chunks + blockIdx.x] = sum;
+    if (sum) atomicAdd(&d->digit_total[0][t], sum);
   }
   // Clearing duties for later kernels (their look-back words and the dense
   // cell map must start empty).
   const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  const int64_t nsweep = (int64_t)p.sweep_tiles * kRadix;
-  for (int64_t i = tid; i < nsweep; i += stride) p.sweep_status[0][i] = 0;
   for (int64_t i = tid; i < p.scan_tiles; i += stride) { p.rle_status[i] = 0; p.ids_status[i] = 0; }
   const int64_t dense = (int64_t)d->dense_total;
   for (int64_t i = tid; i < dense; i += stride) p.cell_map[i] = -1;
 }
 
-// ------------------------------------------------------------- k_onesweep
+// ------------------------------------------------------- radix pass kernels
+// Pass `pass` of the LSD sort over digit (key >> 8*pass) & 255, in three
+// steps that never wait on one another's blocks:
+//   k_sort_count    histogram of the digit per chunk (pass 0: done by k_keys)
+//   k_sort_scan     exclusive scan of the digit-major [digit][chunk] counts:
+//                   where each chunk's run of each digit starts in the output
+//   k_sort_scatter  each chunk, tile by tile: stable warp-match ranking of
+//                   4096 keys in shared memory, staged scatter so that each
+//                   digit run is written contiguously; the last pass writes
+//                   perm and gathers the sorted float2 coordinates
+// Passes at or beyond the device-side pass count return at once.
+template <typename K>
+__device__ __forceinline__ void count_body(const Plan& p, int pass, uint32_t (*h)[kRadix]) {
+  const int64_t n = p.n;
+  const K* keys = reinterpret_cast<const K*>(p.keys[pass & 1]);
+  const int64_t b0 = (int64_t)blockIdx.x * p.chunk_tiles * kSortTile;
+  const int64_t b1 = min(n, b0 + (int64_t)p.chunk_tiles * kSortTile);
+  const uint32_t shift = pass * kRadixBits;
+  const uint32_t warp = threadIdx.x >> 5;
+  for (int64_t i = b0 + threadIdx.x; i < b1; i += blockDim.x)
+    atomicAdd(&h[warp][(uint32_t)((uint64_t)keys[i] >> shift) & (kRadix - 1)], 1u);
+}
+
+__global__ void __launch_bounds__(kSortThreads) k_sort_count(Plan p, int pass) {
+  __shared__ uint32_t h[kSortWarps][kRadix];
+  const Desc* d = p.desc;
+  if (pass >= (int)d->npasses) return;
+  for (int i = threadIdx.x; i < kSortWarps * kRadix; i += blockDim.x) (&h[0][0])[i] = 0;
+  __syncthreads();
+  if (d->key64) count_body<uint64_t>(p, pass, h);
+  else count_body<uint32_t>(p, pass, h);
+  __syncthreads();
+  const uint32_t t = threadIdx.x;
+  uint32_t sum = 0;
+#pragma unroll
+  for (int w = 0; w < kSortWarps; ++w) sum += h[w][t];
+  p.chunk_count[(int64_t)t * p.sort_chunks + blockIdx.x] = sum;
+  if (sum) atomicAdd(&p.desc->digit_total[pass & 1][t], sum);
+}
+
+constexpr int kScanBlock = 1024;  // >= kMaxChunks
+
+// One block per digit: exclusive scan of the digit's row of chunk counts,
+// offset by the total of all lower digits (from the digit totals the count
+// step accumulated). Also clears the totals the next pass will accumulate.
+__global__ void __launch_bounds__(kScanBlock) k_sort_scan(Plan p, int pass) {
+  __shared__ uint32_t s_warp[kScanBlock / 32];
+  __shared__ uint32_t s_base;
+  Desc* d = p.desc;
+  if (pass >= (int)d->npasses) return;
+  const uint32_t dig = blockIdx.x;
+  const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
+  if (warp == 0) {
+    // Total of the digits below `dig`.
+    uint32_t acc = 0;
+    for (uint32_t t = lane; t < dig; t += 32) acc += d->digit_total[pass & 1][t];
+    acc = __reduce_add_sync(0xffffffffu, acc);
+    if (lane == 0) s_base = acc;
+  }
+  uint32_t* row = p.chunk_count + (int64_t)dig * p.sort_chunks;
+  const int32_t b = threadIdx.x;
+  const uint32_t v = b < p.sort_chunks ? row[b] : 0u;
+  uint32_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= (uint32_t)o) x += y;
+  }
+  if (lane == 31) s_warp[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    const uint32_t w = s_warp[lane];
+    uint32_t z = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, z, o);
+      if (lane >= (uint32_t)o) z += y;
+    }
+    s_warp[lane] = z - w;
+  }
+  __syncthreads();
+  if (b < p.sort_chunks) row[b] = s_base + s_warp[warp] + x - v;
+  if (dig == 0 && threadIdx.x < kRadix) d->digit_total[(pass & 1) ^ 1][threadIdx.x] = 0;
+}
+
+__device__ __forceinline__ uint32_t digit_of(uint32_t key, uint32_t shift) {
+  return (key >> shift) & (kRadix - 1);
+}
+__device__ __forceinline__ uint32_t digit_of(uint64_t key, uint32_t shift) {
+  return (uint32_t)(key >> shift) & (kRadix - 1);
+}
+
 struct SweepSmem {
-  uint32_t wcnt[kSortWarps][kRadix];   // per-warp digit counts -> warp offsets
+  uint32_t wcnt[kSortWarps][kRadix + 1];  // per-warp digit counts -> warp offsets
+                                          // (slot kRadix absorbs invalid items)
   uint32_t tile_excl[kRadix];          // exclusive scan of tile digit counts
-  uint32_t glob[kRadix];               // global position of each digit run
-  uint32_t bucket[kRadix];             // exclusive scan of the digit histogram
+  uint32_t glob[kRadix];               // output position of this tile's digit runs
+  uint32_t carry[kRadix];              // next output position of each digit
   uint32_t warp_tot[kSortWarps];
-  uint32_t tile;
 };
 
 template <typename K>
-__device__ __forceinline__ void onesweep_body(const Plan& p, int pass, bool last, SweepSmem& sm,
-                                              unsigned char* stage_raw) {
+__device__ __forceinline__ void scatter_body(const Plan& p, int pass, bool last, SweepSmem& sm,
+                                             unsigned char* stage_raw) {
   const int64_t n = p.n;
   const uint32_t lane = lane_id();
   const uint32_t warp = threadIdx.x >> 5;
@@ -304,78 +398,49 @@ __device__ __forceinline__ void onesweep_body(const Plan& p, int pass, bool last
   uint32_t* vals_out = last ? p.perm : p.vals[src ^ 1];
   K* st_keys = reinterpret_cast<K*>(stage_raw);
   uint32_t* st_vals = reinterpret_cast<uint32_t*>(stage_raw + sizeof(K) * kSortTile);
-  unsigned long long* words = p.sweep_status[pass & 1];
-  Desc* d = p.desc;
 
-  // Bucket bases: exclusive scan of this digit's global histogram.
-  {
-    const uint32_t t = threadIdx.x;
-    uint32_t v = d->hist[pass][t];
-    uint32_t x = v;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-      if (lane >= (uint32_t)o) x += y;
-    }
-    if (lane == 31) sm.warp_tot[warp] = x;
+  sm.carry[threadIdx.x] = p.chunk_count[(int64_t)threadIdx.x * p.sort_chunks + blockIdx.x];
+  const int64_t c0 = (int64_t)blockIdx.x * p.chunk_tiles * kSortTile;
+  const int64_t c1 = min(n, c0 + (int64_t)p.chunk_tiles * kSortTile);
+  for (int64_t tile_base = c0; tile_base < c1; tile_base += kSortTile) {
+    for (int i = threadIdx.x; i < kSortWarps * (kRadix + 1); i += blockDim.x) (&sm.wcnt[0][0])[i] = 0;
     __syncthreads();
-    uint32_t wpre = 0;
-    for (uint32_t w = 0; w < warp; ++w) wpre += sm.warp_tot[w];
-    sm.bucket[t] = wpre + x - v;
-    __syncthreads();
-  }
-
-  // Clear the other look-back region for the next pass.
-  {
-    unsigned long long* other = p.sweep_status[(pass & 1) ^ 1];
-    const int64_t total = (int64_t)p.sweep_tiles * kRadix;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
-         i += (int64_t)gridDim.x * blockDim.x)
-      other[i] = 0;
-  }
-
-  while (true) {
-    if (threadIdx.x == 0) sm.tile = atomicAdd(&d->ctr[kCtrPass0 + pass], 1u);
-    for (int i = threadIdx.x; i < kSortWarps * kRadix; i += blockDim.x) (&sm.wcnt[0][0])[i] = 0;
-    __syncthreads();
-    const uint32_t tile = sm.tile;
-    if ((int64_t)tile >= p.sweep_tiles) break;
-    const int64_t tile_base = (int64_t)tile * kSortTile;
     const int64_t wbase = tile_base + (int64_t)warp * 32 * kSortItems;
-
+    // Keys of this warp's slice in (k, lane) order; digits are recomputed
+    // and values read at staging time to keep few registers live.
     K key[kSortItems];
-    uint32_t val[kSortItems];
-    uint32_t dig[kSortItems];
     uint32_t rank[kSortItems];
 #pragma unroll
     for (int k = 0; k < kSortItems; ++k) {
       const int64_t gi = wbase + k * 32 + lane;
-      if (gi < n) {
-        key[k] = keys_in[gi];
-        val[k] = pass == 0 ? (uint32_t)gi : vals_in[gi];
-        dig[k] = (uint32_t)((uint64_t)key[k] >> shift) & (kRadix - 1);
-      } else {
-        key[k] = 0; val[k] = 0; dig[k] = kRadix;  // sentinel digit
-      }
+      key[k] = gi < c1 ? keys_in[gi] : (K)0;
     }
-    // Stable warp ranking: items in (k, lane) order.
+    // Stable warp ranking in (k, lane) order. Peers (lanes holding the same
+    // digit) come from one ballot per digit bit; the first lane of each peer
+    // group advances the warp's counter for the digit.
+    const uint32_t lt = lanemask_lt();
 #pragma unroll
     for (int k = 0; k < kSortItems; ++k) {
-      const uint32_t dk = dig[k];
-      const uint32_t peers = __match_any_sync(0xffffffffu, dk);
-      const uint32_t leader = __ffs(peers) - 1;
-      uint32_t old = 0;
-      if (lane == leader && dk < kRadix) {
-        old = sm.wcnt[warp][dk];
-        sm.wcnt[warp][dk] = old + __popc(peers);
+      const int64_t gi = wbase + k * 32 + lane;
+      const bool valid = gi < c1;
+      const uint32_t dk = digit_of(key[k], shift);
+      uint32_t peers = __ballot_sync(0xffffffffu, valid);
+      if (!valid) peers = ~peers;
+#pragma unroll
+      for (int b = 0; b < kRadixBits; ++b) {
+        const bool bit = (dk >> b) & 1u;
+        const uint32_t m = __ballot_sync(0xffffffffu, bit);
+        peers &= bit ? m : ~m;
       }
-      old = __shfl_sync(0xffffffffu, old, leader);
-      rank[k] = old + __popc(peers & lanemask_lt());
+      const uint32_t slot = valid ? dk : (uint32_t)kRadix;
+      const uint32_t pre = __popc(peers & lt);
+      const uint32_t old = sm.wcnt[warp][slot];
       __syncwarp();
+      if (pre == 0) sm.wcnt[warp][slot] = old + __popc(peers);
+      __syncwarp();
+      rank[k] = old + pre;
     }
     __syncthreads();
-    // Per digit: warp exclusive offsets and the tile count.
-    uint32_t tile_cnt;
     {
       const uint32_t t = threadIdx.x;
       uint32_t run = 0;
@@ -385,50 +450,38 @@ __device__ __forceinline__ void onesweep_body(const Plan& p, int pass, bool last
         sm.wcnt[w][t] = run;
         run += c;
       }
-      tile_cnt = run;
-      // Publish this tile's aggregate (or inclusive prefix for tile 0).
-      unsigned long long* my = words + (int64_t)tile * kRadix + t;
-      if (tile == 0) st_relaxed(my, kFlagInc | (unsigned long long)tile_cnt);
-      else st_relaxed(my, kFlagAgg | (unsigned long long)tile_cnt);
-      // Block exclusive scan of tile counts over digits.
-      uint32_t x = tile_cnt;
+      uint32_t x = run;
 #pragma unroll
       for (int o = 1; o < 32; o <<= 1) {
-        uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
         if (lane >= (uint32_t)o) x += y;
       }
       if (lane == 31) sm.warp_tot[warp] = x;
       __syncthreads();
       uint32_t wpre = 0;
       for (uint32_t w = 0; w < warp; ++w) wpre += sm.warp_tot[w];
-      sm.tile_excl[t] = wpre + x - tile_cnt;
-      // Look-back for digit t.
-      unsigned long long excl = 0;
-      if (tile > 0) {
-        excl = lookback(words + t, tile, kRadix, d);
-        st_relaxed(my, kFlagInc | (excl + tile_cnt));
-      }
-      sm.glob[t] = sm.bucket[t] + (uint32_t)excl;
+      sm.tile_excl[t] = wpre + x - run;
+      sm.glob[t] = sm.carry[t];
+      sm.carry[t] += run;
     }
     __syncthreads();
-    // Stage into shared memory in tile-sorted order.
 #pragma unroll
     for (int k = 0; k < kSortItems; ++k) {
-      const uint32_t dk = dig[k];
-      if (dk < kRadix) {
+      const int64_t gi = wbase + k * 32 + lane;
+      if (gi < c1) {
+        const uint32_t dk = digit_of(key[k], shift);
         const uint32_t lp = sm.tile_excl[dk] + sm.wcnt[warp][dk] + rank[k];
         st_keys[lp] = key[k];
-        st_vals[lp] = val[k];
+        st_vals[lp] = pass == 0 ? (uint32_t)gi : vals_in[gi];
       }
     }
     __syncthreads();
-    const int32_t valid = (int32_t)min((int64_t)kSortTile, n - tile_base);
+    const int32_t valid = (int32_t)min((int64_t)kSortTile, c1 - tile_base);
     for (int32_t lp = threadIdx.x; lp < valid; lp += blockDim.x) {
       const K kk = st_keys[lp];
-      const uint32_t dk = (uint32_t)((uint64_t)kk >> shift) & (kRadix - 1);
+      const uint32_t dk = digit_of(kk, shift);
       const uint32_t gpos = sm.glob[dk] + (uint32_t)lp - sm.tile_excl[dk];
       const uint32_t vv = st_vals[lp];
-      if ((int64_t)gpos >= n) continue;  // only after a failed look-back
       keys_out[gpos] = kk;
       vals_out[gpos] = vv;
       if (last) p.xy[gpos] = p.X[vv];
@@ -437,7 +490,7 @@ __device__ __forceinline__ void onesweep_body(const Plan& p, int pass, bool last
   }
 }
 
-__global__ void __launch_bounds__(kSortThreads) k_onesweep(Plan p, int pass) {
+__global__ void __launch_bounds__(kSortThreads, 3) k_sort_scatter(Plan p, int pass) {
   extern __shared__ __align__(16) unsigned char dyn_smem[];
   SweepSmem& sm = *reinterpret_cast<SweepSmem*>(dyn_smem);
   unsigned char* stage = dyn_smem + ((sizeof(SweepSmem) + 15) & ~size_t(15));
@@ -445,8 +498,8 @@ __global__ void __launch_bounds__(kSortThreads) k_onesweep(Plan p, int pass) {
   const int np = (int)d->npasses;
   if (pass >= np) return;
   const bool last = pass == np - 1;
-  if (d->key64) onesweep_body<uint64_t>(p, pass, last, sm, stage);
-  else onesweep_body<uint32_t>(p, pass, last, sm, stage);
+  if (d->key64) scatter_body<uint64_t>(p, pass, last, sm, stage);
+  else scatter_body<uint32_t>(p, pass, last, sm, stage);
 }
 
 constexpr size_t kSweepSmemBytes =
@@ -462,29 +515,24 @@ static int grid_for(const Plan& p, int64_t work, int threads, int per_sm) {
 }
 
 cudaError_t launch_front(const Plan& p, cudaStream_t s) {
-  k_init<<<grid_for(p, kMaxPasses * kRadix, 256, 1), 256, 0, s>>>(p);
+  k_init<<<grid_for(p, (int64_t)p.nseg + kNumCtr, 256, 1), 256, 0, s>>>(p);
   k_bounds<<<grid_for(p, p.n, 256 * 8, 8), 256, 0, s>>>(p);
   k_seg_finalize<<<1, 1024, 0, s>>>(p);
-  k_keys_hist<<<grid_for(p, p.n, 256 * 8, 8), 256, 0, s>>>(p);
+  k_keys<<<p.sort_chunks, kSortThreads, 0, s>>>(p);
   return cudaGetLastError();
 }
 
 cudaError_t launch_sort_pass(const Plan& p, int pass, cudaStream_t s) {
   static bool attr_set = false;
   if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(k_onesweep, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(k_sort_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)kSweepSmemBytes);
     if (e != cudaSuccess) return e;
     attr_set = true;
   }
-  // Persistent grid: blocks loop over tiles taken from an atomic counter.
-  int blocks_per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_onesweep, kSortThreads,
-                                                kSweepSmemBytes);
-  if (blocks_per_sm < 1) blocks_per_sm = 1;
-  int grid = p.num_sms * blocks_per_sm;
-  if (grid > p.sweep_tiles) grid = p.sweep_tiles > 0 ? p.sweep_tiles : 1;
-  k_onesweep<<<grid, kSortThreads, kSweepSmemBytes, s>>>(p, pass);
+  if (pass > 0) k_sort_count<<<p.sort_chunks, kSortThreads, 0, s>>>(p, pass);
+  k_sort_scan<<<kRadix, kScanBlock, 0, s>>>(p, pass);
+  k_sort_scatter<<<p.sort_chunks, kSortThreads, kSweepSmemBytes, s>>>(p, pass);
   return cudaGetLastError();
 }
 
