@@ -70,6 +70,9 @@ size_t carve(int64_t n, int32_t nseg, char* base, Plan* p) {
   q.big_base = cv.take<unsigned long long>((size_t)q.big_cap);
   q.big_done = cv.take<uint32_t>((size_t)q.big_cap);
   q.big_chunk_box = cv.take<float4>((size_t)q.chunk_cap);
+  q.bin_count = cv.take<uint32_t>((size_t)q.dense_cap);
+  q.blk_sum = cv.take<uint32_t>((size_t)kMaxGrid);
+  q.blk_ne = cv.take<uint32_t>((size_t)kMaxGrid);
   q.n = n;
   q.nseg = nseg;
   q.scan_tiles = scan_tiles;
@@ -134,8 +137,9 @@ int run_pipeline(const Plan& p, cudaStream_t s, cudaEvent_t* evs) {
   if ((e = mark(0)) != cudaSuccess) return to_code(e);
   if ((e = launch_front(p, s)) != cudaSuccess) return to_code(e);            // cell_keys
   if ((e = mark(1)) != cudaSuccess) return to_code(e);
-  for (int pass = 0; pass < kMaxPasses; ++pass)                               // sort_gather
-    if ((e = launch_sort_pass(p, pass, s)) != cudaSuccess) return to_code(e);
+  if ((e = launch_csort(p, s)) != cudaSuccess) return to_code(e);            // sort_gather
+  if ((e = launch_keys(p, s)) != cudaSuccess) return to_code(e);
+  if ((e = launch_radix(p, s)) != cudaSuccess) return to_code(e);
   if ((e = mark(2)) != cudaSuccess) return to_code(e);
   if ((e = launch_rle(p, s)) != cudaSuccess) return to_code(e);              // boundary_scan
   if ((e = mark(3)) != cudaSuccess) return to_code(e);
@@ -272,6 +276,7 @@ int dbs_dbscan2d_debug(const float* X, int64_t n, double eps, int64_t min_sample
   int rc = prepare_single(X, n, eps, min_samples, labels, ws, ws_bytes, &p);
   if (rc != DBS_OK || n == 0) return rc;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  p.force_radix = 1;  // stable sort: perm and sorted coordinates as the reference's
   rc = run_pipeline(p, s, nullptr);
   if (rc != DBS_OK) return rc;
   rc = run_debug_export(p, *out, s, n);

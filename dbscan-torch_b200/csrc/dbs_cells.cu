@@ -100,6 +100,7 @@ __device__ __forceinline__ void rle_body(const Plan& p, K* s_keys, uint32_t* s_w
         ++c;
       }
       p.point_cell[i] = (int32_t)max((int64_t)0, min((int64_t)c - 1, n - 1));
+      p.xy[i] = p.X[p.perm[i]];  // the reference's k_gather_xy
     }
     __syncthreads();
   }
@@ -110,6 +111,7 @@ __global__ void __launch_bounds__(kScanThreads) k_rle(Plan p) {
   __shared__ uint32_t s_warp[kScanThreads / 32];
   __shared__ uint32_t s_tile;
   __shared__ unsigned long long s_excl;
+  if (p.desc->dense_sort) return;  // cells came from the counting sort
   if (p.desc->key64)
     rle_body<uint64_t>(p, reinterpret_cast<uint64_t*>(s_raw), s_warp, &s_tile, &s_excl);
   else
@@ -154,13 +156,16 @@ __global__ void __launch_bounds__(kCellThreads) k_cell_prep(Plan p) {
     if (valid) { s0 = p.cell_start[c]; s1 = p.cell_start[c + 1]; }
     const bool big = valid && (s1 - s0) > kBigCell;
     if (valid && !big) {
-      // A one-point cell keeps its raw coordinates: the reference seeds the
-      // fold with xs[s] and flushes subnormals only through fminf/fmaxf.
+      // Gather the cell's sorted coordinates (the reference's k_gather_xy),
+      // record each point's cell, fold the box. A one-point cell keeps its
+      // raw coordinates: the reference seeds the fold with xs[s] and flushes
+      // subnormals only through fminf/fmaxf.
       float2 v = p.xy[s0];
       float4 b = make_float4(v.x, v.x, v.y, v.y);
       if (s1 - s0 > 1) {
-        b = make_float4(INFINITY, -INFINITY, INFINITY, -INFINITY);
-        for (int32_t i = s0; i < s1; ++i) {
+        b = make_float4(fminf(v.x, INFINITY), fmaxf(v.x, -INFINITY), fminf(v.y, INFINITY),
+                        fmaxf(v.y, -INFINITY));
+        for (int32_t i = s0 + 1; i < s1; ++i) {
           v = p.xy[i];
           b.x = fminf(b.x, v.x); b.y = fmaxf(b.y, v.x);
           b.z = fminf(b.z, v.y); b.w = fmaxf(b.w, v.y);

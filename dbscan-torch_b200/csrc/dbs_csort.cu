@@ -1,0 +1,228 @@
+// dbs_csort.cu -- counting sort of points by cell over a dense key space.
+//
+// Reference path replaced (ryanirl/dbscan-torch v0.2.0, csrc/cuda/dbscan_cuda.cu):
+//   k_cell_keys :55-66, thrust::sort_by_key :582-586, k_gather_xy :71-79,
+//   k_boundary_flags / inclusive_scan / k_extract_cell_start :84-120 and the
+//   host read of num_cells :612-617.
+//
+// When every cloud's compacted key range is dense (at most 4N + 4096 keys,
+// the same rule that gives a cloud a dense cell map), the sort needs no
+// radix passes: a key *is* its bin. One cooperative kernel, phases separated
+// by grid barriers:
+//   0. clear the per-key counters
+//   1. count points per key (warp-aggregated atomics: a 2M-point cell costs
+//      one atomic per warp, not per point)
+//   2. per-block sums of counts and non-empty keys over contiguous key ranges
+//   3. exclusive scan of the block sums (block 0)
+//   4. rescan each range: the counter becomes the key's first output
+//      position, the dense cell map gets each non-empty key's cell index, and
+//      the cells get cell_start / cell_key / cell_seg (the run-length cells of
+//      the reference, in the same ascending key order, without a pass over
+//      sorted keys)
+//   5. scatter every point's index and cell to its key's next slot (perm,
+//      point_cell: 4-byte writes)
+//   6. gather the sorted float2 coordinates point-parallel (coalesced writes)
+// Points inside one cell land in arrival order rather than input order. No
+// label depends on that order (core counts, cell-pair edges, boxes and the
+// (d2, input index) border rule are all order-free), and cell indices are
+// key ranks, identical to the reference's; only the debug entry point, which
+// returns perm, forces the stable radix sort.
+#include "dbs_internal.cuh"
+
+namespace dbs {
+
+constexpr int kCsThreads = 256;
+constexpr uint32_t kFullMask = 0xffffffffu;
+
+// Global key of point i of cloud seg (dense mode: fits 31 bits).
+__device__ __forceinline__ uint32_t dense_key(const Plan& p, int64_t i, int32_t seg) {
+  const SegInfo& g = p.seg_info[seg];
+  const float inv_r = p.seg_param[seg].inv_r;
+  const float2 v = p.X[i];
+  const uint64_t gx = compact_axis(cell_coord(v.x, inv_r), g.bx, g.px);
+  const uint64_t gy = compact_axis(cell_coord(v.y, inv_r), g.by, g.py);
+  return (uint32_t)(g.base + (gx << g.ysh) + gy);
+}
+
+// Cloud owning global key b: the last cloud whose key base is <= b (empty
+// clouds share their base with the next cloud and come before it).
+__device__ __forceinline__ int32_t seg_of_key(const Plan& p, uint64_t b) {
+  if (p.nseg == 1) return 0;
+  int32_t lo = 0, hi = p.nseg - 1;
+  while (lo < hi) {
+    const int32_t mid = (lo + hi + 1) >> 1;
+    if (p.seg_info[mid].base <= b) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Block-wide exclusive scan of two counters; returns the block totals.
+__device__ __forceinline__ void block_scan2(uint32_t a, uint32_t b, uint32_t& xa, uint32_t& xb,
+                                            uint32_t& ta, uint32_t& tb, uint32_t* s_a, uint32_t* s_b) {
+  const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
+  const int nw = blockDim.x >> 5;
+  uint32_t ia = a, ib = b;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t ya = __shfl_up_sync(kFullMask, ia, o);
+    const uint32_t yb = __shfl_up_sync(kFullMask, ib, o);
+    if (lane >= (uint32_t)o) { ia += ya; ib += yb; }
+  }
+  if (lane == 31) { s_a[warp] = ia; s_b[warp] = ib; }
+  __syncthreads();
+  uint32_t pa = 0, pb = 0;
+  ta = 0; tb = 0;
+  for (int w = 0; w < nw; ++w) {
+    if (w < (int)warp) { pa += s_a[w]; pb += s_b[w]; }
+    ta += s_a[w]; tb += s_b[w];
+  }
+  xa = pa + ia - a;
+  xb = pb + ib - b;
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(kCsThreads) k_csort(Plan p) {
+  __shared__ uint32_t s_a[kCsThreads / 32], s_b[kCsThreads / 32];
+  Desc* d = p.desc;
+  if (!d->dense_sort) return;
+  const int64_t n = p.n;
+  const int64_t W = (int64_t)d->dense_total;
+  uint32_t* bins = p.bin_count;
+  const uint32_t lane = lane_id();
+  const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t nthr = (int64_t)gridDim.x * blockDim.x;
+
+  // 0. clear counters
+  for (int64_t b = tid; b < W; b += nthr) bins[b] = 0;
+  grid_sync(&d->bar, d);
+
+  // 1. count (warp-uniform loop; peers = lanes with the same key)
+  {
+    const int64_t wstart = tid - lane;
+    int32_t seg = seg_of(p, min(wstart + lane, n > 0 ? n - 1 : 0));
+    for (int64_t base = wstart; base < n; base += nthr) {
+      const int64_t i = base + lane;
+      const bool valid = i < n;
+      uint32_t key = 0xffffffffu;
+      if (valid) {
+        while (i >= p.seg_off[seg + 1]) ++seg;
+        key = dense_key(p, i, seg);
+      }
+      const uint32_t peers = __match_any_sync(kFullMask, key);
+      if (valid && lane == (uint32_t)(__ffs(peers) - 1)) atomicAdd(&bins[key], (uint32_t)__popc(peers));
+    }
+  }
+  grid_sync(&d->bar, d);
+
+  // 2. block range sums
+  const int64_t per = (W + gridDim.x - 1) / gridDim.x;
+  const int64_t r0 = min(W, (int64_t)blockIdx.x * per), r1 = min(W, r0 + per);
+  {
+    uint32_t cs = 0, ne = 0;
+    for (int64_t b = r0 + threadIdx.x; b < r1; b += blockDim.x) {
+      const uint32_t c = bins[b];
+      cs += c;
+      ne += c != 0;
+    }
+    uint32_t xa, xb, ta, tb;
+    block_scan2(cs, ne, xa, xb, ta, tb, s_a, s_b);
+    if (threadIdx.x == 0) { p.blk_sum[blockIdx.x] = ta; p.blk_ne[blockIdx.x] = tb; }
+  }
+  grid_sync(&d->bar, d);
+
+  // 3. exclusive scan of block sums (block 0; gridDim.x <= kMaxGrid)
+  if (blockIdx.x == 0) {
+    const int per_t = (gridDim.x + blockDim.x - 1) / blockDim.x;
+    const int a0 = threadIdx.x * per_t, a1 = min((int)gridDim.x, a0 + per_t);
+    uint32_t cs = 0, ne = 0;
+    for (int k = a0; k < a1; ++k) { cs += p.blk_sum[k]; ne += p.blk_ne[k]; }
+    uint32_t xa, xb, ta, tb;
+    block_scan2(cs, ne, xa, xb, ta, tb, s_a, s_b);
+    for (int k = a0; k < a1; ++k) {
+      const uint32_t c = p.blk_sum[k], e = p.blk_ne[k];
+      p.blk_sum[k] = xa;
+      p.blk_ne[k] = xb;
+      xa += c;
+      xb += e;
+    }
+    if (threadIdx.x == 0) {
+      d->num_cells = tb;
+      p.cell_start[tb] = (int32_t)n;
+    }
+  }
+  grid_sync(&d->bar, d);
+
+  // 4. rescan: offsets, dense cell map, cells
+  {
+    uint32_t carry_cs = p.blk_sum[blockIdx.x], carry_ne = p.blk_ne[blockIdx.x];
+    for (int64_t cb = r0; cb < r1; cb += blockDim.x) {
+      const int64_t b = cb + threadIdx.x;
+      const uint32_t c = b < r1 ? bins[b] : 0u;
+      const uint32_t f = c != 0;
+      uint32_t xa, xb, ta, tb;
+      block_scan2(c, f, xa, xb, ta, tb, s_a, s_b);
+      if (b < r1) {
+        const uint32_t off = carry_cs + xa;
+        const uint32_t cell = carry_ne + xb;
+        bins[b] = off;
+        p.cell_map[b] = f ? (int32_t)cell : -1;
+        const int32_t sg = seg_of_key(p, (uint64_t)b);
+        if ((uint64_t)b == p.seg_info[sg].base) p.seg_info[sg].cell_begin = (int32_t)cell;
+        if (f) {
+          p.cell_start[cell] = (int32_t)off;
+          p.cell_key[cell] = (uint64_t)b;
+          p.cell_seg[cell] = sg;
+        }
+      }
+      carry_cs += ta;
+      carry_ne += tb;
+    }
+  }
+  grid_sync(&d->bar, d);
+
+  // 5. scatter
+  {
+    const uint32_t lt = lanemask_lt();
+    const int64_t wstart = tid - lane;
+    int32_t seg = seg_of(p, min(wstart + lane, n > 0 ? n - 1 : 0));
+    for (int64_t base = wstart; base < n; base += nthr) {
+      const int64_t i = base + lane;
+      const bool valid = i < n;
+      uint32_t key = 0xffffffffu;
+      if (valid) {
+        while (i >= p.seg_off[seg + 1]) ++seg;
+        key = dense_key(p, i, seg);
+      }
+      const uint32_t peers = __match_any_sync(kFullMask, key);
+      const uint32_t leader = __ffs(peers) - 1;
+      uint32_t pos = 0;
+      if (valid && lane == leader) pos = atomicAdd(&bins[key], (uint32_t)__popc(peers));
+      pos = __shfl_sync(kFullMask, pos, leader) + __popc(peers & lt);
+      if (valid) {
+        p.perm[pos] = (uint32_t)i;
+        p.point_cell[pos] = p.cell_map[key];
+      }
+    }
+  }
+  grid_sync(&d->bar, d);
+
+  // 6. gather the sorted coordinates (the reference's k_gather_xy):
+  //    coalesced perm reads and xy writes, independent random reads of X.
+  for (int64_t i = tid; i < n; i += nthr) p.xy[i] = p.X[p.perm[i]];
+}
+
+cudaError_t launch_csort(const Plan& p, cudaStream_t s) {
+  static int blocks_per_sm = 0;
+  if (blocks_per_sm == 0) {
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_csort, kCsThreads, 0);
+    if (e != cudaSuccess) return e;
+    if (blocks_per_sm < 1) return cudaErrorLaunchOutOfResources;
+  }
+  int grid = p.num_sms * blocks_per_sm;
+  if (grid > kMaxGrid) grid = kMaxGrid;
+  Plan q = p;
+  void* args[] = {&q};
+  return cudaLaunchCooperativeKernel((const void*)k_csort, dim3(grid), dim3(kCsThreads), args, 0, s);
+}
+
+}  // namespace dbs

@@ -37,6 +37,7 @@ constexpr int kSortWarps = kSortThreads / 32;
 constexpr int kSortItems = 16;
 constexpr int kSortTile = kSortThreads * kSortItems;
 constexpr int kMaxChunks = 1024;
+constexpr int kMaxGrid = 4096;   // blocks of a cooperative launch (bound)
 constexpr int kScanThreads = 256;
 constexpr int kScanItems = 16;
 constexpr int kScanTile = kScanThreads * kScanItems;
@@ -57,6 +58,7 @@ enum : uint32_t {
   kErrLookback = 1u << 0,   // a decoupled look-back wait hit its cap
   kErrFind = 1u << 1,       // a union-find walk / hook loop hit its cap
   kErrKeySpace = 1u << 2,   // batched key ranges overflow 64 bits
+  kErrBarrier = 1u << 3,    // a grid barrier wait hit its cap
 };
 
 // Dynamic work counters (Desc::ctr).
@@ -99,6 +101,12 @@ struct SegInfo {
   uint32_t ysh;      // bits of the y part of the local key
 };
 
+// Software grid barrier of the cooperative kernels (all blocks resident).
+struct GridBar {
+  unsigned int count;
+  unsigned int gen;
+};
+
 struct Desc {
   uint32_t status;
   uint32_t key64;      // keys stored as u64 (else u32)
@@ -110,6 +118,9 @@ struct Desc {
   unsigned long long big_packed;  // huge cells: entries << 40 | chunks
   uint32_t ctr[kNumCtr];
   uint32_t digit_total[2][kRadix];  // per-pass digit totals (ping-pong)
+  uint32_t dense_sort;  // 1: counting sort over the dense key space
+  uint32_t pad1;
+  GridBar bar;
 };
 
 // Device pointers of one call, carved out of the caller's workspace.
@@ -145,6 +156,10 @@ struct Plan {
   float4* big_chunk_box;  // bounding box of each chunk
   int64_t big_cap;        // entries available in big_cell
   int64_t chunk_cap;      // entries available in big_chunk_box
+  uint32_t* bin_count;    // counting sort: per-key counts -> offsets -> cursors
+  uint32_t* blk_sum;      // counting sort: per-block bin sums (kMaxGrid)
+  uint32_t* blk_ne;       // counting sort: per-block non-empty bin counts
+  int32_t force_radix;    // debug entry: stable radix sort (reference perm)
   int64_t n;
   int32_t nseg;
   int32_t sort_chunks;    // chunks of the radix passes (one block each)
@@ -273,10 +288,42 @@ __device__ __forceinline__ unsigned long long lookback(const unsigned long long*
   return excl;
 }
 
+__device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int* p) {
+  unsigned int v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Grid-wide barrier for cooperative launches. Bounded: a wait past
+// kSpinCap polls sets kErrBarrier and returns (the kernel then finishes with
+// invalid results rather than hanging).
+__device__ __forceinline__ void grid_sync(GridBar* b, Desc* d) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned int g = ld_acquire_u32(&b->gen);
+    __threadfence();
+    if (atomicAdd(&b->count, 1u) == gridDim.x - 1) {
+      atomicExch(&b->count, 0u);
+      __threadfence();
+      atomicAdd(&b->gen, 1u);
+    } else {
+      uint32_t spins = 0;
+      while (ld_acquire_u32(&b->gen) == g) {
+        if (++spins > kSpinCap) { set_error(d, kErrBarrier); break; }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+}
+
 // --------------------------------------------------------- host launchers
 // Each returns cudaGetLastError() of its launches.
 cudaError_t launch_front(const Plan& p, cudaStream_t s);      // init, bounds, finalize, keys
-cudaError_t launch_sort_pass(const Plan& p, int pass, cudaStream_t s);
+cudaError_t launch_keys(const Plan& p, cudaStream_t s);
+cudaError_t launch_radix(const Plan& p, cudaStream_t s);
+cudaError_t launch_csort(const Plan& p, cudaStream_t s);
 cudaError_t launch_rle(const Plan& p, cudaStream_t s);
 cudaError_t launch_cell_prep(const Plan& p, cudaStream_t s);
 cudaError_t launch_core(const Plan& p, cudaStream_t s);

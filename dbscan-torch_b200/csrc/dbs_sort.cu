@@ -41,6 +41,8 @@ __global__ void k_init(Plan p) {
     d->big_packed = 0;
   }
   for (int64_t i = tid; i < 2 * kRadix; i += stride) (&d->digit_total[0][0])[i] = 0;
+  if (tid == 0) { d->bar.count = 0; d->bar.gen = 0; d->dense_sort = 0; }
+  for (int64_t i = tid; i < p.scan_tiles; i += stride) { p.rle_status[i] = 0; p.ids_status[i] = 0; }
   if (p.single && tid == 0) {
     p.seg_off[0] = 0;
     p.seg_off[1] = p.n;
@@ -153,8 +155,8 @@ __global__ void __launch_bounds__(1024) k_seg_finalize(Plan p) {
   __shared__ unsigned long long s_range[1024];
   __shared__ unsigned long long s_dense[1024];
   __shared__ unsigned long long s_carry_range, s_carry_dense;
-  __shared__ int s_overflow;
-  if (threadIdx.x == 0) { s_carry_range = 0; s_carry_dense = 0; s_overflow = 0; }
+  __shared__ int s_overflow, s_sparse;
+  if (threadIdx.x == 0) { s_carry_range = 0; s_carry_dense = 0; s_overflow = 0; s_sparse = 0; }
   __syncthreads();
   for (int32_t s0 = 0; s0 < p.nseg; s0 += blockDim.x) {
     const int32_t s = s0 + threadIdx.x;
@@ -176,6 +178,7 @@ __global__ void __launch_bounds__(1024) k_seg_finalize(Plan p) {
         else range = g.wx << g.ysh;
         const unsigned long long cap = (unsigned long long)(kDenseFactor * npts + kDenseSlack);
         if (!sat && range <= cap) dense = range;
+        else atomicOr(&s_sparse, 1);
       }
     }
     s_range[threadIdx.x] = range;
@@ -230,6 +233,9 @@ __global__ void __launch_bounds__(1024) k_seg_finalize(Plan p) {
     unsigned long long dt = s_carry_dense;
     if ((long long)dt > p.dense_cap) dt = 0;  // cannot happen by construction
     d->dense_total = dt;
+    // Counting sort when every non-empty cloud is dense (then the global key
+    // of a point is its dense-map index) and keys fit 31 bits.
+    d->dense_sort = (!p.force_radix && !s_sparse && !s_overflow && dt < (1ull << 31)) ? 1u : 0u;
     if (s_overflow) set_error(d, kErrKeySpace);
   }
 }
@@ -261,6 +267,7 @@ __device__ __forceinline__ void keys_body(const Plan& p, uint32_t (*h)[kRadix]) 
 __global__ void __launch_bounds__(kSortThreads) k_keys(Plan p) {
   __shared__ uint32_t h[kSortWarps][kRadix];
   Desc* d = p.desc;
+  if (d->dense_sort) return;
   for (int i = threadIdx.x; i < kSortWarps * kRadix; i += blockDim.x) (&h[0][0])[i] = 0;
   __syncthreads();
   if (d->key64) keys_body<uint64_t>(p, h);
@@ -278,74 +285,62 @@ __global__ void __launch_bounds__(kSortThreads) k_keys(Plan p) {
   // cell map must start empty).
   const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t i = tid; i < p.scan_tiles; i += stride) { p.rle_status[i] = 0; p.ids_status[i] = 0; }
   const int64_t dense = (int64_t)d->dense_total;
   for (int64_t i = tid; i < dense; i += stride) p.cell_map[i] = -1;
 }
 
-// ------------------------------------------------------- radix pass kernels
-// Pass `pass` of the LSD sort over digit (key >> 8*pass) & 255, in three
-// steps that never wait on one another's blocks:
-//   k_sort_count    histogram of the digit per chunk (pass 0: done by k_keys)
-//   k_sort_scan     exclusive scan of the digit-major [digit][chunk] counts:
-//                   where each chunk's run of each digit starts in the output
-//   k_sort_scatter  each chunk, tile by tile: stable warp-match ranking of
-//                   4096 keys in shared memory, staged scatter so that each
-//                   digit run is written contiguously; the last pass writes
-//                   perm and gathers the sorted float2 coordinates
-// Passes at or beyond the device-side pass count return at once.
+// ------------------------------------------------------- radix sort kernel
+// The LSD sort for key spaces too wide for the counting sort (and for the
+// debug entry point, whose perm must be stable): one cooperative kernel runs
+// every pass the device-side pass count asks for, each pass as three phases
+// separated by grid barriers (no unused passes, no extra launches):
+//   count    histogram of the digit per chunk (pass 0: done by k_keys)
+//   scan     per digit, exclusive scan of its row of chunk counts, offset by
+//            the total of all lower digits
+//   scatter  each chunk, tile by tile: stable ranking of 4096 keys in shared
+//            memory, staged scatter so each digit run is written
+//            contiguously; the last pass writes perm and gathers the sorted
+//            float2 coordinates
 template <typename K>
-__device__ __forceinline__ void count_body(const Plan& p, int pass, uint32_t (*h)[kRadix]) {
+__device__ __forceinline__ void count_body(const Plan& p, int pass, int32_t chunk, uint32_t (*h)[kRadix]) {
   const int64_t n = p.n;
   const K* keys = reinterpret_cast<const K*>(p.keys[pass & 1]);
-  const int64_t b0 = (int64_t)blockIdx.x * p.chunk_tiles * kSortTile;
+  const int64_t b0 = (int64_t)chunk * p.chunk_tiles * kSortTile;
   const int64_t b1 = min(n, b0 + (int64_t)p.chunk_tiles * kSortTile);
   const uint32_t shift = pass * kRadixBits;
   const uint32_t warp = threadIdx.x >> 5;
-  for (int64_t i = b0 + threadIdx.x; i < b1; i += blockDim.x)
-    atomicAdd(&h[warp][(uint32_t)((uint64_t)keys[i] >> shift) & (kRadix - 1)], 1u);
-}
-
-__global__ void __launch_bounds__(kSortThreads) k_sort_count(Plan p, int pass) {
-  __shared__ uint32_t h[kSortWarps][kRadix];
-  const Desc* d = p.desc;
-  if (pass >= (int)d->npasses) return;
   for (int i = threadIdx.x; i < kSortWarps * kRadix; i += blockDim.x) (&h[0][0])[i] = 0;
   __syncthreads();
-  if (d->key64) count_body<uint64_t>(p, pass, h);
-  else count_body<uint32_t>(p, pass, h);
+  for (int64_t i = b0 + threadIdx.x; i < b1; i += blockDim.x)
+    atomicAdd(&h[warp][(uint32_t)((uint64_t)keys[i] >> shift) & (kRadix - 1)], 1u);
   __syncthreads();
   const uint32_t t = threadIdx.x;
   uint32_t sum = 0;
 #pragma unroll
   for (int w = 0; w < kSortWarps; ++w) sum += h[w][t];
-  p.chunk_count[(int64_t)t * p.sort_chunks + blockIdx.x] = sum;
+  p.chunk_count[(int64_t)t * p.sort_chunks + chunk] = sum;
   if (sum) atomicAdd(&p.desc->digit_total[pass & 1][t], sum);
+  __syncthreads();
 }
 
-constexpr int kScanBlock = 1024;  // >= kMaxChunks
-
-// One block per digit: exclusive scan of the digit's row of chunk counts,
-// offset by the total of all lower digits (from the digit totals the count
-// step accumulated). Also clears the totals the next pass will accumulate.
-__global__ void __launch_bounds__(kScanBlock) k_sort_scan(Plan p, int pass) {
-  __shared__ uint32_t s_warp[kScanBlock / 32];
-  __shared__ uint32_t s_base;
+// Exclusive scan of digit `dig`'s row of chunk counts (sort_chunks <=
+// kMaxChunks = 4 * kSortThreads entries), offset by the total of the lower
+// digits.
+__device__ __forceinline__ void scan_body(const Plan& p, int pass, uint32_t dig, uint32_t* s_warp) {
   Desc* d = p.desc;
-  if (pass >= (int)d->npasses) return;
-  const uint32_t dig = blockIdx.x;
   const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
-  if (warp == 0) {
-    // Total of the digits below `dig`.
-    uint32_t acc = 0;
-    for (uint32_t t = lane; t < dig; t += 32) acc += d->digit_total[pass & 1][t];
-    acc = __reduce_add_sync(0xffffffffu, acc);
-    if (lane == 0) s_base = acc;
-  }
+  uint32_t base = 0;
+  for (uint32_t t = lane; t < dig; t += 32) base += d->digit_total[pass & 1][t];
+  base = __reduce_add_sync(0xffffffffu, base);
   uint32_t* row = p.chunk_count + (int64_t)dig * p.sort_chunks;
-  const int32_t b = threadIdx.x;
-  const uint32_t v = b < p.sort_chunks ? row[b] : 0u;
-  uint32_t x = v;
+  const int32_t b0 = threadIdx.x * 4;
+  uint32_t v[4], sum = 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    v[k] = b0 + k < p.sort_chunks ? row[b0 + k] : 0u;
+    sum += v[k];
+  }
+  uint32_t x = sum;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
     const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
@@ -353,19 +348,14 @@ __global__ void __launch_bounds__(kScanBlock) k_sort_scan(Plan p, int pass) {
   }
   if (lane == 31) s_warp[warp] = x;
   __syncthreads();
-  if (warp == 0) {
-    const uint32_t w = s_warp[lane];
-    uint32_t z = w;
+  uint32_t run = base + x - sum;
+  for (uint32_t w = 0; w < warp; ++w) run += s_warp[w];
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t y = __shfl_up_sync(0xffffffffu, z, o);
-      if (lane >= (uint32_t)o) z += y;
-    }
-    s_warp[lane] = z - w;
+  for (int k = 0; k < 4; ++k) {
+    if (b0 + k < p.sort_chunks) row[b0 + k] = run;
+    run += v[k];
   }
   __syncthreads();
-  if (b < p.sort_chunks) row[b] = s_base + s_warp[warp] + x - v;
-  if (dig == 0 && threadIdx.x < kRadix) d->digit_total[(pass & 1) ^ 1][threadIdx.x] = 0;
 }
 
 __device__ __forceinline__ uint32_t digit_of(uint32_t key, uint32_t shift) {
@@ -382,11 +372,15 @@ struct SweepSmem {
   uint32_t glob[kRadix];               // output position of this tile's digit runs
   uint32_t carry[kRadix];              // next output position of each digit
   uint32_t warp_tot[kSortWarps];
+  uint32_t warp_tot_wide[kSortWarps];
+  __device__ uint32_t (*wcnt_as_hist())[kRadix] {
+    return reinterpret_cast<uint32_t (*)[kRadix]>(&wcnt[0][0]);
+  }
 };
 
 template <typename K>
-__device__ __forceinline__ void scatter_body(const Plan& p, int pass, bool last, SweepSmem& sm,
-                                             unsigned char* stage_raw) {
+__device__ __forceinline__ void scatter_body(const Plan& p, int pass, bool last, int32_t chunk,
+                                             SweepSmem& sm, unsigned char* stage_raw) {
   const int64_t n = p.n;
   const uint32_t lane = lane_id();
   const uint32_t warp = threadIdx.x >> 5;
@@ -399,8 +393,8 @@ __device__ __forceinline__ void scatter_body(const Plan& p, int pass, bool last,
   K* st_keys = reinterpret_cast<K*>(stage_raw);
   uint32_t* st_vals = reinterpret_cast<uint32_t*>(stage_raw + sizeof(K) * kSortTile);
 
-  sm.carry[threadIdx.x] = p.chunk_count[(int64_t)threadIdx.x * p.sort_chunks + blockIdx.x];
-  const int64_t c0 = (int64_t)blockIdx.x * p.chunk_tiles * kSortTile;
+  sm.carry[threadIdx.x] = p.chunk_count[(int64_t)threadIdx.x * p.sort_chunks + chunk];
+  const int64_t c0 = (int64_t)chunk * p.chunk_tiles * kSortTile;
   const int64_t c1 = min(n, c0 + (int64_t)p.chunk_tiles * kSortTile);
   for (int64_t tile_base = c0; tile_base < c1; tile_base += kSortTile) {
     for (int i = threadIdx.x; i < kSortWarps * (kRadix + 1); i += blockDim.x) (&sm.wcnt[0][0])[i] = 0;
@@ -484,22 +478,39 @@ __device__ __forceinline__ void scatter_body(const Plan& p, int pass, bool last,
       const uint32_t vv = st_vals[lp];
       keys_out[gpos] = kk;
       vals_out[gpos] = vv;
-      if (last) p.xy[gpos] = p.X[vv];
     }
     __syncthreads();
   }
 }
 
-__global__ void __launch_bounds__(kSortThreads, 3) k_sort_scatter(Plan p, int pass) {
+__global__ void __launch_bounds__(kSortThreads, 3) k_radix(Plan p) {
   extern __shared__ __align__(16) unsigned char dyn_smem[];
   SweepSmem& sm = *reinterpret_cast<SweepSmem*>(dyn_smem);
   unsigned char* stage = dyn_smem + ((sizeof(SweepSmem) + 15) & ~size_t(15));
-  const Desc* d = p.desc;
+  Desc* d = p.desc;
+  if (d->dense_sort) return;
   const int np = (int)d->npasses;
-  if (pass >= np) return;
-  const bool last = pass == np - 1;
-  if (d->key64) scatter_body<uint64_t>(p, pass, last, sm, stage);
-  else scatter_body<uint32_t>(p, pass, last, sm, stage);
+  const bool wide = d->key64 != 0;
+  for (int pass = 0; pass < np; ++pass) {
+    if (pass > 0) {
+      for (int32_t ch = blockIdx.x; ch < p.sort_chunks; ch += gridDim.x) {
+        if (wide) count_body<uint64_t>(p, pass, ch, sm.wcnt_as_hist());
+        else count_body<uint32_t>(p, pass, ch, sm.wcnt_as_hist());
+      }
+      grid_sync(&d->bar, d);
+    }
+    for (uint32_t dig = blockIdx.x; dig < (uint32_t)kRadix; dig += gridDim.x)
+      scan_body(p, pass, dig, sm.warp_tot_wide);
+    if (blockIdx.x == 0)
+      for (int t = threadIdx.x; t < kRadix; t += blockDim.x) d->digit_total[(pass & 1) ^ 1][t] = 0;
+    grid_sync(&d->bar, d);
+    const bool last = pass == np - 1;
+    for (int32_t ch = blockIdx.x; ch < p.sort_chunks; ch += gridDim.x) {
+      if (wide) scatter_body<uint64_t>(p, pass, last, ch, sm, stage);
+      else scatter_body<uint32_t>(p, pass, last, ch, sm, stage);
+    }
+    if (pass + 1 < np) grid_sync(&d->bar, d);
+  }
 }
 
 constexpr size_t kSweepSmemBytes =
@@ -515,25 +526,35 @@ static int grid_for(const Plan& p, int64_t work, int threads, int per_sm) {
 }
 
 cudaError_t launch_front(const Plan& p, cudaStream_t s) {
-  k_init<<<grid_for(p, (int64_t)p.nseg + kNumCtr, 256, 1), 256, 0, s>>>(p);
+  k_init<<<grid_for(p, (int64_t)p.nseg + p.scan_tiles + 2 * kRadix, 256, 2), 256, 0, s>>>(p);
   k_bounds<<<grid_for(p, p.n, 256 * 8, 8), 256, 0, s>>>(p);
   k_seg_finalize<<<1, 1024, 0, s>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_keys(const Plan& p, cudaStream_t s) {
   k_keys<<<p.sort_chunks, kSortThreads, 0, s>>>(p);
   return cudaGetLastError();
 }
 
-cudaError_t launch_sort_pass(const Plan& p, int pass, cudaStream_t s) {
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(k_sort_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
+// Cooperative launch: every block of the grid must be resident for the grid
+// barriers, so the grid is the occupancy-derived number of resident blocks.
+cudaError_t launch_radix(const Plan& p, cudaStream_t s) {
+  static int blocks_per_sm = 0;
+  if (blocks_per_sm == 0) {
+    cudaError_t e = cudaFuncSetAttribute(k_radix, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)kSweepSmemBytes);
     if (e != cudaSuccess) return e;
-    attr_set = true;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_radix, kSortThreads,
+                                                      kSweepSmemBytes);
+    if (e != cudaSuccess) return e;
+    if (blocks_per_sm < 1) return cudaErrorLaunchOutOfResources;
   }
-  if (pass > 0) k_sort_count<<<p.sort_chunks, kSortThreads, 0, s>>>(p, pass);
-  k_sort_scan<<<kRadix, kScanBlock, 0, s>>>(p, pass);
-  k_sort_scatter<<<p.sort_chunks, kSortThreads, kSweepSmemBytes, s>>>(p, pass);
-  return cudaGetLastError();
+  const int grid = p.num_sms * blocks_per_sm;
+  Plan q = p;
+  void* args[] = {&q};
+  return cudaLaunchCooperativeKernel((const void*)k_radix, dim3(grid), dim3(kSortThreads), args,
+                                     kSweepSmemBytes, s);
 }
 
 }  // namespace dbs

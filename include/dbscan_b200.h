@@ -48,6 +48,7 @@ extern "C" {
 #define DBS_STATUS_LOOKBACK 1u  /* a decoupled look-back wait reached its cap */
 #define DBS_STATUS_FIND 2u      /* a union-find walk reached its cap */
 #define DBS_STATUS_KEYSPACE 4u  /* batched cell-key ranges overflowed 64 bits */
+#define DBS_STATUS_BARRIER 8u   /* a grid-wide barrier wait reached its cap */
 
 #define DBS_NUM_STAGES 10
 
