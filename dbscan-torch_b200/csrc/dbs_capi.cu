@@ -62,6 +62,9 @@ size_t carve(int64_t n, int32_t nseg, char* base, Plan* p) {
   q.cell_status = cv.take<uint8_t>(N);
   q.uf = cv.take<int32_t>(N);
   q.root_rank = cv.take<int32_t>(N);
+  q.cid = cv.take<int32_t>(N);
+  q.qlist = cv.take<uint32_t>(N);
+  q.blist = cv.take<uint32_t>(N);
   q.dense_cap = kDenseFactor * (int64_t)N + kDenseSlack * (int64_t)nseg;
   q.cell_map = cv.take<int32_t>((size_t)q.dense_cap);
   q.big_cap = (int64_t)(N / kHugeCell) + 1;
@@ -191,8 +194,7 @@ __global__ void k_debug_export(Plan p, dbs_debug_buffers o) {
     c = __shfl_sync(0xffffffffu, c, 0);
     if (c >= C) break;
     const int32_t seg = p.cell_seg[c];
-    const int32_t seg_roots = p.root_rank[p.seg_info[seg].cell_begin];
-    const int32_t cid = p.cell_status[c] == 0 ? -1 : p.root_rank[p.uf[c]] - seg_roots;
+    const int32_t cid = p.cid[c];
     if (lane == 0 && o.cluster_id_per_cell) o.cluster_id_per_cell[c] = cid;
     const float inv_r = p.seg_param[seg].inv_r;
     for (int32_t i = p.cell_start[c] + lane; i < p.cell_start[c + 1]; i += 32) {

@@ -99,7 +99,6 @@ __device__ __forceinline__ void rle_body(const Plan& p, K* s_keys, uint32_t* s_w
         }
         ++c;
       }
-      p.point_cell[i] = (int32_t)max((int64_t)0, min((int64_t)c - 1, n - 1));
       p.xy[i] = p.X[p.perm[i]];  // the reference's k_gather_xy
     }
     __syncthreads();
@@ -161,11 +160,13 @@ __global__ void __launch_bounds__(kCellThreads) k_cell_prep(Plan p) {
       // raw coordinates: the reference seeds the fold with xs[s] and flushes
       // subnormals only through fminf/fmaxf.
       float2 v = p.xy[s0];
+      p.point_cell[s0] = (int32_t)c;
       float4 b = make_float4(v.x, v.x, v.y, v.y);
       if (s1 - s0 > 1) {
         b = make_float4(fminf(v.x, INFINITY), fmaxf(v.x, -INFINITY), fminf(v.y, INFINITY),
                         fmaxf(v.y, -INFINITY));
         for (int32_t i = s0 + 1; i < s1; ++i) {
+          p.point_cell[i] = (int32_t)c;
           v = p.xy[i];
           b.x = fminf(b.x, v.x); b.y = fmaxf(b.y, v.x);
           b.z = fminf(b.z, v.y); b.w = fmaxf(b.w, v.y);
@@ -190,8 +191,10 @@ __global__ void __launch_bounds__(kCellThreads) k_cell_prep(Plan p) {
       const int l = __ffs(bm) - 1;
       bm &= bm - 1;
       const int32_t b0 = __shfl_sync(full, s0, l), b1 = __shfl_sync(full, s1, l);
+      const int32_t cl = (int32_t)__shfl_sync(full, c, l);
       float xmin = INFINITY, xmax = -INFINITY, ymin = INFINITY, ymax = -INFINITY;
       for (int32_t i = b0 + lane; i < b1; i += 32) {
+        p.point_cell[i] = cl;
         const float2 v = p.xy[i];
         xmin = fminf(xmin, v.x); xmax = fmaxf(xmax, v.x);
         ymin = fminf(ymin, v.y); ymax = fmaxf(ymax, v.y);
@@ -262,6 +265,7 @@ __global__ void __launch_bounds__(256) k_huge_bbox(Plan p) {
     const int32_t a = s0 + k * kHugeChunk, b = min(s1, a + kHugeChunk);
     float xmin = INFINITY, xmax = -INFINITY, ymin = INFINITY, ymax = -INFINITY;
     for (int32_t i = a + lane; i < b; i += 32) {
+      p.point_cell[i] = c;
       const float2 v = p.xy[i];
       xmin = fminf(xmin, v.x); xmax = fmaxf(xmax, v.x);
       ymin = fminf(ymin, v.y); ymax = fmaxf(ymax, v.y);
@@ -310,7 +314,7 @@ cudaError_t launch_rle(const Plan& p, cudaStream_t s) {
 }
 
 cudaError_t launch_cell_prep(const Plan& p, cudaStream_t s) {
-  k_cell_prep<<<p.num_sms * 4, kCellThreads, 0, s>>>(p);
+  k_cell_prep<<<p.num_sms * 8, kCellThreads, 0, s>>>(p);
   k_huge_bbox<<<p.num_sms * 4, 256, 0, s>>>(p);
   return cudaGetLastError();
 }

@@ -21,38 +21,75 @@ constexpr uint32_t kFull = 0xffffffffu;
 
 
 // ----------------------------------------------------------------- k_core
-// Core flag of every sorted point, one thread per point. A point of a cell
-// with >= ms points is core wholesale (k_core_pass1). Otherwise it counts its
+// Warp-aggregated append of the lanes with `take` to a work list.
+__device__ __forceinline__ void append(uint32_t* list, uint32_t* count, bool take, uint32_t v) {
+  const uint32_t m = __ballot_sync(kFull, take);
+  if (m == 0) return;
+  const uint32_t lane = lane_id();
+  uint32_t base = 0;
+  if (lane == 0) base = atomicAdd(count, (uint32_t)__popc(m));
+  base = __shfl_sync(kFull, base, 0);
+  if (take) list[base + __popc(m & lanemask_lt())] = v;
+}
+
+// Point classification, one thread per sorted point: a point of a cell with
+// >= ms points is core wholesale (k_core_pass1, dbscan_cuda.cu:199-208);
+// every other point goes to the query list of k_core, so that k_core's warps
+// hold only points with a neighbour scan to do.
+__global__ void __launch_bounds__(256) k_classify(Plan p) {
+  const int64_t n = p.n;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < n; base += stride) {
+    const int64_t i = base + threadIdx.x;
+    bool query = false;
+    if (i < n) {
+      const int32_t c = p.point_cell[i];
+      if (p.cell_start[c + 1] - p.cell_start[c] >= p.seg_param[p.cell_seg[c]].ms) p.is_core[i] = 1;
+      else query = true;
+    }
+    append(p.qlist, &p.desc->q_count, query, (uint32_t)i);
+  }
+}
+
+// Core flag of every query point, one thread per query. A query counts its
 // own cell wholesale (the reference never distance-tests the centre cell,
 // :231-233) plus the points within eps of the other 24 stencil cells that
-// survive the point-box prune (:235-240), stopping once the count reaches ms.
-// Threads of one warp are consecutive points, mostly of one cell, so the
-// neighbour row, boxes and candidate points are shared loads.
+// survive the point-box prune (:235-240), stopping once the count reaches
+// ms (k_core_pass2 :213-245). Queries that stay non-core go to the border
+// list of k_labels.
 __global__ void __launch_bounds__(kCellThreads) k_core(Plan p) {
-  const int64_t n = p.n;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    const int32_t c = p.point_cell[i];
-    const int32_t st0 = p.cell_start[c], st1 = p.cell_start[c + 1];
-    const SegParam sp = p.seg_param[p.cell_seg[c]];
-    const int32_t ms = sp.ms;
-    int32_t cnt = st1 - st0;
-    if (cnt >= ms) { p.is_core[i] = 1; continue; }
-    const float eps_sq = sp.eps_sq;
-    const float2 q = p.xy[i];
-    const int32_t* row = p.ngh + (int64_t)c * kNgh;
-    for (int off = 0; off < kNgh && cnt < ms; ++off) {
-      if (off == 12) continue;
-      const int32_t nb = row[off];
-      if (nb < 0) continue;
-      if (!(point_box_d2(q.x, q.y, p.bbox[nb]) <= eps_sq)) continue;
-      const int32_t j1 = p.cell_start[nb + 1];
-      for (int32_t j = p.cell_start[nb]; j < j1; ++j) {
-        const float2 pj = p.xy[j];
-        cnt += sq_dist(__fsub_rn(pj.x, q.x), __fsub_rn(pj.y, q.y)) <= eps_sq;
+  const uint32_t qn = p.desc->q_count;
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t base = blockIdx.x * blockDim.x; base < qn; base += stride) {
+    const uint32_t t = base + threadIdx.x;
+    bool noncore = false;
+    uint32_t i = 0;
+    if (t < qn) {
+      i = p.qlist[t];
+      const int32_t c = p.point_cell[i];
+      const int32_t st0 = p.cell_start[c], st1 = p.cell_start[c + 1];
+      const SegParam sp = p.seg_param[p.cell_seg[c]];
+      const int32_t ms = sp.ms;
+      const float eps_sq = sp.eps_sq;
+      int32_t cnt = st1 - st0;
+      const float2 q = p.xy[i];
+      const int32_t* row = p.ngh + (int64_t)c * kNgh;
+      for (int off = 0; off < kNgh && cnt < ms; ++off) {
+        if (off == 12) continue;
+        const int32_t nb = row[off];
+        if (nb < 0) continue;
+        if (!(point_box_d2(q.x, q.y, p.bbox[nb]) <= eps_sq)) continue;
+        const int32_t j1 = p.cell_start[nb + 1];
+        for (int32_t j = p.cell_start[nb]; j < j1; ++j) {
+          const float2 pj = p.xy[j];
+          cnt += sq_dist(__fsub_rn(pj.x, q.x), __fsub_rn(pj.y, q.y)) <= eps_sq;
+        }
       }
+      const bool core = cnt >= ms;
+      p.is_core[i] = core ? 1 : 0;
+      noncore = !core;
     }
-    p.is_core[i] = cnt >= ms ? 1 : 0;
+    append(p.blist, &p.desc->b_count, noncore, i);
   }
 }
 
@@ -334,25 +371,39 @@ __global__ void __launch_bounds__(kScanThreads) k_ids(Plan p) {
   }
 }
 
+// ---------------------------------------------------------------- k_cid
+// Cluster id of every cell: the rank of its root among its cloud's roots
+// (k_cluster_id_per_cell, dbscan_cuda.cu:392-404), -1 for cells without a
+// core point.
+__global__ void __launch_bounds__(256) k_cid(Plan p) {
+  const uint32_t C = p.desc->num_cells;
+  for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < C; c += gridDim.x * blockDim.x) {
+    int32_t id = -1;
+    if (p.cell_status[c] != 0)
+      id = p.root_rank[p.uf[c]] - p.root_rank[p.seg_info[p.cell_seg[c]].cell_begin];
+    p.cid[c] = id;
+  }
+}
+
 // --------------------------------------------------------------- k_labels
-// Final label of every sorted point, written straight to input order
-// (k_core_labels :409-417, k_border_assign :427-470, k_unpermute :475-481).
-// A core point takes its cell's cluster id: the rank of the cell's root
-// among the roots of its cloud. A non-core point takes the cluster of the
-// core point within eps that minimises (d2, input index) over the 25 stencil
-// cells with a core point, pruned by the point-box test; -1 when none.
+// Final labels, written straight to input order (k_core_labels :409-417,
+// k_border_assign :427-470, k_unpermute :475-481). Items [0, b_count) are
+// the non-core points of the border list: each takes the cluster of the
+// core point within eps that minimises (d2, input index) over the 25
+// stencil cells with a core point, pruned by the point-box test, or -1.
+// Items after that are all sorted points; core ones take their cell's id.
 __global__ void __launch_bounds__(kCellThreads) k_labels(Plan p) {
   const int64_t n = p.n;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    const int32_t c = p.point_cell[i];
-    const int32_t seg = p.cell_seg[c];
-    const int32_t seg_roots = p.root_rank[p.seg_info[seg].cell_begin];
+  const int64_t bn = p.desc->b_count;
+  const int64_t total = bn + n;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t i;
     int32_t lab;
-    if (p.is_core[i]) {
-      lab = p.root_rank[p.uf[c]] - seg_roots;
-    } else {
-      const float eps_sq = p.seg_param[seg].eps_sq;
+    if (t < bn) {
+      i = p.blist[t];
+      const int32_t c = p.point_cell[i];
+      const float eps_sq = p.seg_param[p.cell_seg[c]].eps_sq;
       const float2 q = p.xy[i];
       const int32_t* row = p.ngh + (int64_t)c * kNgh;
       unsigned long long best = ~0ull;
@@ -373,7 +424,11 @@ __global__ void __launch_bounds__(kCellThreads) k_labels(Plan p) {
           }
         }
       }
-      lab = best_nb < 0 ? -1 : p.root_rank[p.uf[best_nb]] - seg_roots;
+      lab = best_nb < 0 ? -1 : p.cid[best_nb];
+    } else {
+      i = t - bn;
+      if (!p.is_core[i]) continue;
+      lab = p.cid[p.point_cell[i]];
     }
     p.labels[p.perm[i]] = lab;
   }
@@ -381,6 +436,7 @@ __global__ void __launch_bounds__(kCellThreads) k_labels(Plan p) {
 
 // ------------------------------------------------------------- launchers
 cudaError_t launch_core(const Plan& p, cudaStream_t s) {
+  k_classify<<<p.num_sms * 8, 256, 0, s>>>(p);
   k_core<<<p.num_sms * 8, kCellThreads, 0, s>>>(p);
   k_status<<<p.num_sms * 8, 256, 0, s>>>(p);
   return cudaGetLastError();
@@ -399,6 +455,7 @@ cudaError_t launch_ids(const Plan& p, cudaStream_t s) {
 }
 
 cudaError_t launch_labels(const Plan& p, cudaStream_t s) {
+  k_cid<<<p.num_sms * 4, 256, 0, s>>>(p);
   k_labels<<<p.num_sms * 8, kCellThreads, 0, s>>>(p);
   return cudaGetLastError();
 }

@@ -10,8 +10,8 @@
 // radix passes: a key *is* its bin. One cooperative kernel, phases separated
 // by grid barriers:
 //   0. clear the per-key counters
-//   1. count points per key (warp-aggregated atomics: a 2M-point cell costs
-//      one atomic per warp, not per point)
+//   1. count points per key (atomics aggregated over lanes with equal keys,
+//      so a 2M-point cell costs about one atomic per warp, not per point)
 //   2. per-block sums of counts and non-empty keys over contiguous key ranges
 //   3. exclusive scan of the block sums (block 0)
 //   4. rescan each range: the counter becomes the key's first output
@@ -19,8 +19,7 @@
 //      the cells get cell_start / cell_key / cell_seg (the run-length cells of
 //      the reference, in the same ascending key order, without a pass over
 //      sorted keys)
-//   5. scatter every point's index and cell to its key's next slot (perm,
-//      point_cell: 4-byte writes)
+//   5. scatter every point's index to its key's next slot (perm)
 //   6. gather the sorted float2 coordinates point-parallel (coalesced writes)
 // Points inside one cell land in arrival order rather than input order. No
 // label depends on that order (core counts, cell-pair edges, boxes and the
@@ -34,14 +33,47 @@ namespace dbs {
 constexpr int kCsThreads = 256;
 constexpr uint32_t kFullMask = 0xffffffffu;
 
-// Global key of point i of cloud seg (dense mode: fits 31 bits).
-__device__ __forceinline__ uint32_t dense_key(const Plan& p, int64_t i, int32_t seg) {
+// Global key of point v of cloud seg (dense mode: fits 31 bits).
+__device__ __forceinline__ uint32_t dense_key(const Plan& p, float2 v, int32_t seg) {
   const SegInfo& g = p.seg_info[seg];
   const float inv_r = p.seg_param[seg].inv_r;
-  const float2 v = p.X[i];
   const uint64_t gx = compact_axis(cell_coord(v.x, inv_r), g.bx, g.px);
   const uint64_t gy = compact_axis(cell_coord(v.y, inv_r), g.by, g.py);
   return (uint32_t)(g.base + (gx << g.ysh) + gy);
+}
+
+// Points per lane and iteration of the point loops: independent loads and
+// atomics in flight per thread.
+constexpr int kU = 4;
+
+// Warp aggregation of equal keys for the per-key atomics. __match_any_sync
+// groups lanes with equal keys, but its cost grows with the number of
+// distinct keys in the warp (about 7x a plain atomic's issue cost for 32
+// distinct keys on B200). A warp first checks for duplicates between lanes
+// l and l^16: warps of mostly distinct keys (the common case) skip the match
+// and use one atomic per lane; warps with duplicates (a dense cell holding a
+// large share of the points) group them so each key costs one atomic.
+struct Agg {
+  uint32_t group;   // lanes sharing this lane's atomic (bit set = member)
+  uint32_t leader;  // lane that issues it
+};
+
+__device__ __forceinline__ Agg aggregate(uint32_t key, bool valid) {
+  const uint32_t lane = lane_id();
+  const uint32_t k = valid ? key : 0xffffffffu;
+  // Every lane takes part in the shuffle (no short-circuit around a
+  // warp-synchronous call).
+  const uint32_t other = __shfl_xor_sync(kFullMask, k, 16);
+  const bool dup = valid && k == other;
+  Agg a;
+  if (__ballot_sync(kFullMask, dup) == 0) {
+    a.group = 1u << lane;
+    a.leader = lane;
+  } else {
+    a.group = __match_any_sync(kFullMask, k);
+    a.leader = __ffs(a.group) - 1;
+  }
+  return a;
 }
 
 // Cloud owning global key b: the last cloud whose key base is <= b (empty
@@ -93,26 +125,39 @@ __global__ void __launch_bounds__(kCsThreads) k_csort(Plan p) {
   const int64_t nthr = (int64_t)gridDim.x * blockDim.x;
 
   // 0. clear counters
+  mark_phase(d, 0);
   for (int64_t b = tid; b < W; b += nthr) bins[b] = 0;
   grid_sync(&d->bar, d);
+  mark_phase(d, 1);
 
-  // 1. count (warp-uniform loop; peers = lanes with the same key)
+  // 1. count. Each warp takes kU consecutive 32-point rows per iteration;
+  // peers = lanes with the same key, one atomic per peer group.
+  const int64_t gwarp = tid >> 5, nwarps = nthr >> 5;
   {
-    const int64_t wstart = tid - lane;
-    int32_t seg = seg_of(p, min(wstart + lane, n > 0 ? n - 1 : 0));
-    for (int64_t base = wstart; base < n; base += nthr) {
-      const int64_t i = base + lane;
-      const bool valid = i < n;
-      uint32_t key = 0xffffffffu;
-      if (valid) {
-        while (i >= p.seg_off[seg + 1]) ++seg;
-        key = dense_key(p, i, seg);
+    int32_t seg = seg_of(p, min(gwarp * 32 * kU + lane, n > 0 ? n - 1 : 0));
+    for (int64_t base = gwarp * 32 * kU; base < n; base += nwarps * 32 * kU) {
+      float2 v[kU];
+#pragma unroll
+      for (int k = 0; k < kU; ++k) {
+        const int64_t i = base + k * 32 + lane;
+        v[k] = i < n ? p.X[i] : make_float2(0.f, 0.f);
       }
-      const uint32_t peers = __match_any_sync(kFullMask, key);
-      if (valid && lane == (uint32_t)(__ffs(peers) - 1)) atomicAdd(&bins[key], (uint32_t)__popc(peers));
+#pragma unroll
+      for (int k = 0; k < kU; ++k) {
+        const int64_t i = base + k * 32 + lane;
+        const bool valid = i < n;
+        uint32_t key = 0xffffffffu;
+        if (valid) {
+          while (i >= p.seg_off[seg + 1]) ++seg;
+          key = dense_key(p, v[k], seg);
+        }
+        const Agg a = aggregate(key, valid);
+        if (valid && lane == a.leader) atomicAdd(&bins[key], (uint32_t)__popc(a.group));
+      }
     }
   }
   grid_sync(&d->bar, d);
+  mark_phase(d, 2);
 
   // 2. block range sums
   const int64_t per = (W + gridDim.x - 1) / gridDim.x;
@@ -129,6 +174,7 @@ __global__ void __launch_bounds__(kCsThreads) k_csort(Plan p) {
     if (threadIdx.x == 0) { p.blk_sum[blockIdx.x] = ta; p.blk_ne[blockIdx.x] = tb; }
   }
   grid_sync(&d->bar, d);
+  mark_phase(d, 3);
 
   // 3. exclusive scan of block sums (block 0; gridDim.x <= kMaxGrid)
   if (blockIdx.x == 0) {
@@ -151,6 +197,7 @@ __global__ void __launch_bounds__(kCsThreads) k_csort(Plan p) {
     }
   }
   grid_sync(&d->bar, d);
+  mark_phase(d, 4);
 
   // 4. rescan: offsets, dense cell map, cells
   {
@@ -179,36 +226,61 @@ __global__ void __launch_bounds__(kCsThreads) k_csort(Plan p) {
     }
   }
   grid_sync(&d->bar, d);
+  mark_phase(d, 5);
 
   // 5. scatter
   {
     const uint32_t lt = lanemask_lt();
-    const int64_t wstart = tid - lane;
-    int32_t seg = seg_of(p, min(wstart + lane, n > 0 ? n - 1 : 0));
-    for (int64_t base = wstart; base < n; base += nthr) {
-      const int64_t i = base + lane;
-      const bool valid = i < n;
-      uint32_t key = 0xffffffffu;
-      if (valid) {
-        while (i >= p.seg_off[seg + 1]) ++seg;
-        key = dense_key(p, i, seg);
+    int32_t seg = seg_of(p, min(gwarp * 32 * kU + lane, n > 0 ? n - 1 : 0));
+    for (int64_t base = gwarp * 32 * kU; base < n; base += nwarps * 32 * kU) {
+      float2 v[kU];
+#pragma unroll
+      for (int k = 0; k < kU; ++k) {
+        const int64_t i = base + k * 32 + lane;
+        v[k] = i < n ? p.X[i] : make_float2(0.f, 0.f);
       }
-      const uint32_t peers = __match_any_sync(kFullMask, key);
-      const uint32_t leader = __ffs(peers) - 1;
-      uint32_t pos = 0;
-      if (valid && lane == leader) pos = atomicAdd(&bins[key], (uint32_t)__popc(peers));
-      pos = __shfl_sync(kFullMask, pos, leader) + __popc(peers & lt);
-      if (valid) {
-        p.perm[pos] = (uint32_t)i;
-        p.point_cell[pos] = p.cell_map[key];
+      uint32_t pos[kU];
+      Agg ag[kU];
+#pragma unroll
+      for (int k = 0; k < kU; ++k) {
+        const int64_t i = base + k * 32 + lane;
+        uint32_t key = 0xffffffffu;
+        if (i < n) {
+          while (i >= p.seg_off[seg + 1]) ++seg;
+          key = dense_key(p, v[k], seg);
+        }
+        ag[k] = aggregate(key, i < n);
+        pos[k] = 0;
+        if (i < n && lane == ag[k].leader) pos[k] = atomicAdd(&bins[key], (uint32_t)__popc(ag[k].group));
+      }
+#pragma unroll
+      for (int k = 0; k < kU; ++k) {
+        const int64_t i = base + k * 32 + lane;
+        const uint32_t at = __shfl_sync(kFullMask, pos[k], ag[k].leader) + __popc(ag[k].group & lt);
+        if (i < n) p.perm[at] = (uint32_t)i;
       }
     }
   }
   grid_sync(&d->bar, d);
+  mark_phase(d, 6);
 
   // 6. gather the sorted coordinates (the reference's k_gather_xy):
   //    coalesced perm reads and xy writes, independent random reads of X.
-  for (int64_t i = tid; i < n; i += nthr) p.xy[i] = p.X[p.perm[i]];
+  for (int64_t i0 = tid; i0 < n; i0 += nthr * kU) {
+    uint32_t src[kU];
+#pragma unroll
+    for (int k = 0; k < kU; ++k) {
+      const int64_t i = i0 + k * nthr;
+      src[k] = i < n ? p.perm[i] : 0u;
+    }
+#pragma unroll
+    for (int k = 0; k < kU; ++k) {
+      const int64_t i = i0 + k * nthr;
+      if (i < n) p.xy[i] = p.X[src[k]];
+    }
+  }
+  __syncthreads();
+  mark_phase(d, 7);
 }
 
 cudaError_t launch_csort(const Plan& p, cudaStream_t s) {

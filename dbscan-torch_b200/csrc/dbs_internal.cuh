@@ -44,6 +44,7 @@ constexpr int kScanTile = kScanThreads * kScanItems;
 constexpr int kCellThreads = 256;               // warp-per-cell kernels
 constexpr uint32_t kSpinCap = 1u << 22;         // bounded waits (look-back polls)
 constexpr uint32_t kFindCap = 1u << 20;         // bounded union-find walks / retries
+constexpr uint32_t kBarrierCap = 1u << 18;      // bounded grid-barrier polls (~0.1 s)
 constexpr int kNgh = 25;
 constexpr int32_t kHugeCell = 4096;   // cells whose box is reduced by many warps
 constexpr int32_t kHugeChunk = 2048;  // points per chunk of a huge cell
@@ -119,8 +120,14 @@ struct Desc {
   uint32_t ctr[kNumCtr];
   uint32_t digit_total[2][kRadix];  // per-pass digit totals (ping-pong)
   uint32_t dense_sort;  // 1: counting sort over the dense key space
+  uint32_t q_count;     // core-query list length (points of cells below ms)
+  uint32_t b_count;     // border list length (non-core points)
   uint32_t pad1;
   GridBar bar;
+  // %globaltimer (ns) at each phase boundary of the cooperative kernels,
+  // written by block 0 after each grid barrier: a per-phase split readable
+  // from the workspace without a profiler.
+  unsigned long long phase_ns[16];
 };
 
 // Device pointers of one call, carved out of the caller's workspace.
@@ -148,6 +155,9 @@ struct Plan {
   uint8_t* cell_status;   // (n) 0 none, 1 mixed, 2 all core
   int32_t* uf;            // (n)
   int32_t* root_rank;     // (n) exclusive scan of root flags
+  int32_t* cid;           // (n) cluster id per cell
+  uint32_t* qlist;        // (n) sorted positions needing a core count
+  uint32_t* blist;        // (n) sorted positions of non-core points
   int32_t* cell_map;      // dense cell map
   int64_t dense_cap;      // entries available in cell_map
   int32_t* big_cell;      // huge cells (> kHugeCell points): cell index
@@ -297,6 +307,16 @@ __device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int* p) {
 // Grid-wide barrier for cooperative launches. Bounded: a wait past
 // kSpinCap polls sets kErrBarrier and returns (the kernel then finishes with
 // invalid results rather than hanging).
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ void mark_phase(Desc* d, int k) {
+  if (blockIdx.x == 0 && threadIdx.x == 0 && k < 16) d->phase_ns[k] = global_ns();
+}
+
 __device__ __forceinline__ void grid_sync(GridBar* b, Desc* d) {
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -309,7 +329,7 @@ __device__ __forceinline__ void grid_sync(GridBar* b, Desc* d) {
     } else {
       uint32_t spins = 0;
       while (ld_acquire_u32(&b->gen) == g) {
-        if (++spins > kSpinCap) { set_error(d, kErrBarrier); break; }
+        if (++spins > kBarrierCap) { set_error(d, kErrBarrier); break; }
         __nanosleep(64);
       }
     }
