@@ -65,6 +65,11 @@ size_t carve(int64_t n, int32_t nseg, char* base, Plan* p) {
   q.cid = cv.take<int32_t>(N);
   q.qlist = cv.take<uint32_t>(N);
   q.blist = cv.take<uint32_t>(N);
+  // Candidate pairs (c, nc > c) of one ring: each unordered neighbour pair
+  // is listed once, so at most 4 per cell in ring 1 and 8 in ring 2.
+  q.pair_cap = 8 * (int64_t)N;
+  q.plist = cv.take<int2>((size_t)q.pair_cap);
+  q.dlist = cv.take<uint32_t>((size_t)q.pair_cap);
   q.dense_cap = kDenseFactor * (int64_t)N + kDenseSlack * (int64_t)nseg;
   q.cell_map = cv.take<int32_t>((size_t)q.dense_cap);
   q.big_cap = (int64_t)(N / kHugeCell) + 1;

@@ -217,51 +217,85 @@ __constant__ int8_t kRingOffs[2][16] = {
     {6, 7, 8, 11, 13, 16, 17, 18, 0, 0, 0, 0, 0, 0, 0, 0},
     {0, 1, 2, 3, 4, 5, 9, 10, 14, 15, 19, 20, 21, 22, 23, 24}};
 
-// Edges of the cell graph from core cell c to its neighbours nc > c at the
-// offsets of one ring, one thread per (cell, offset). A thread scans its
-// pair serially (i over c's core points passing the point-box prune against
-// nc, j over nc's core points, early exit on the first pair within eps);
-// pairs that exhaust the thread's budget are scanned by the whole warp
-// afterwards (pair_scan). Found edges are united at once. With
-// `skip_united`, a pair already in one component (read-only finds) is not
-// scanned. Whether an edge exists does not depend on the order of the tests,
-// and the components (rooted at their smallest cell) do not depend on the
-// order of the unions, so running ring 1 first and ring 2 after a flatten
-// (when most dense cells are already connected) changes only the work.
-__global__ void __launch_bounds__(kCellThreads) k_union(Plan p, int ring, int skip_united) {
-  const uint32_t lane = lane_id();
+// Edges of the cell graph, in three compacted steps per ring (ring 1 =
+// |dx|, |dy| <= 1; ring 2 = the rest of the 5x5 stencil, run after a
+// flatten so that most of its pairs are already connected):
+//   k_pairs       one thread per core cell: its neighbours nc > c of the
+//                 ring that are core cells and pass the box-box prune
+//                 (dbscan_cuda.cu:329-351); with `skip_united` pairs already
+//                 in one component (read-only finds) are dropped. Survivors
+//                 go to a pair list.
+//   k_pair_scan   one thread per listed pair: i over c's core points passing
+//                 the point-box prune against nc, j over nc's core points,
+//                 early exit on the first pair within eps (:353-368); found
+//                 edges are united (high root hooked under low, :301-311).
+//                 Pairs that exhaust kPairBudget tests go to a second list.
+//   k_pair_warp   one warp per over-budget pair (pair_scan).
+// Whether an edge exists does not depend on the order of the tests, and the
+// components (rooted at their smallest cell) do not depend on the order of
+// the unions, so the labels are those of the reference.
+__global__ void __launch_bounds__(256) k_pairs(Plan p, int ring, int skip_united) {
   Desc* d = p.desc;
   const uint32_t C = d->num_cells;
   const int nofs = ring == 0 ? 8 : 16;
-  const int64_t total = (int64_t)C * nofs;
-  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t base = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; base < total;
-       base += nwarps * 32) {
-    const int64_t t = base + lane;
-    int32_t c = 0, nb = -1;
-    bool cand = false;
-    float eps_sq = 0.f;
-    float4 bb_c = make_float4(0.f, 0.f, 0.f, 0.f), bb_n = bb_c;
-    if (t < total) {
-      c = (int32_t)(t / nofs);
-      const int off = kRingOffs[ring][t - (int64_t)c * nofs];
-      if (p.cell_status[c] != 0) {
-        nb = p.ngh[(int64_t)c * kNgh + off];
-        if (nb > c && p.cell_status[nb] != 0) {
-          eps_sq = p.seg_param[p.cell_seg[c]].eps_sq;
-          bb_c = p.bbox[c];
-          bb_n = p.bbox[nb];
-          cand = box_box_d2(bb_c, bb_n) <= eps_sq;
-          if (cand && skip_united) cand = uf_find_ro(p.uf, c, d) != uf_find_ro(p.uf, nb, d);
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t base = blockIdx.x * blockDim.x; base < C; base += stride) {
+    const uint32_t c = base + threadIdx.x;
+    uint32_t mask = 0;  // candidate offsets (bit k = kRingOffs[ring][k])
+    const int32_t* row = p.ngh + (int64_t)min(c, C - 1) * kNgh;
+    if (c < C && p.cell_status[c] != 0) {
+      const float eps_sq = p.seg_param[p.cell_seg[c]].eps_sq;
+      const float4 bb_c = p.bbox[c];
+      int32_t root_c = -1;
+#pragma unroll
+      for (int k = 0; k < 16; ++k) {
+        if (k >= nofs) continue;
+        const int32_t nb = row[kRingOffs[ring][k]];
+        if (nb <= (int32_t)c || p.cell_status[nb] == 0) continue;
+        if (!(box_box_d2(bb_c, p.bbox[nb]) <= eps_sq)) continue;
+        if (skip_united) {
+          if (root_c < 0) root_c = uf_find_ro(p.uf, (int32_t)c, d);
+          if (uf_find_ro(p.uf, nb, d) == root_c) continue;
         }
+        mask |= 1u << k;
       }
     }
-    bool found = false, deferred = false;
-    int32_t c0 = 0, c1 = 0;
-    if (cand) {
-      c0 = p.cell_start[c];
-      c1 = p.cell_start[c + 1];
+    // Warp-aggregated append of a variable number of pairs per lane.
+    const uint32_t cnt = __popc(mask);
+    uint32_t x = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(kFull, x, o);
+      if (lane_id() >= (uint32_t)o) x += y;
+    }
+    const uint32_t tot = __shfl_sync(kFull, x, 31);
+    uint32_t at = 0;
+    if (lane_id() == 31 && tot) at = atomicAdd(&d->p_count, tot);
+    at = __shfl_sync(kFull, at, 31) + x - cnt;
+    while (mask) {
+      const int k = __ffs(mask) - 1;
+      mask &= mask - 1;
+      if (at < p.pair_cap) p.plist[at] = make_int2((int32_t)c, row[kRingOffs[ring][k]]);
+      ++at;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(256) k_pair_scan(Plan p) {
+  Desc* d = p.desc;
+  const uint32_t np = min(d->p_count, (uint32_t)p.pair_cap);
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t base = blockIdx.x * blockDim.x; base < np; base += stride) {
+    const uint32_t t = base + threadIdx.x;
+    bool deferred = false;
+    if (t < np) {
+      const int2 pr = p.plist[t];
+      const int32_t c = pr.x, nb = pr.y;
+      const float eps_sq = p.seg_param[p.cell_seg[c]].eps_sq;
+      const float4 bb_n = p.bbox[nb];
+      const int32_t c0 = p.cell_start[c], c1 = p.cell_start[c + 1];
       const int32_t n0 = p.cell_start[nb], n1 = p.cell_start[nb + 1];
+      bool found = false;
       int32_t budget = kPairBudget;
       for (int32_t i = c0; i < c1 && !found && !deferred; ++i) {
         if (!p.is_core[i]) continue;
@@ -274,24 +308,25 @@ __global__ void __launch_bounds__(kCellThreads) k_union(Plan p, int ring, int sk
           if (sq_dist(__fsub_rn(pj.x, pi.x), __fsub_rn(pj.y, pi.y)) <= eps_sq) { found = true; break; }
         }
       }
+      if (found) uf_unite(p.uf, c, nb, d);
     }
-    if (found) uf_unite(p.uf, c, nb, d);
-    uint32_t dm = __ballot_sync(kFull, deferred);
-    while (dm) {
-      const int l = __ffs(dm) - 1;
-      dm &= dm - 1;
-      const int32_t cc = __shfl_sync(kFull, c, l);
-      const int32_t nc = __shfl_sync(kFull, nb, l);
-      const float e2 = __shfl_sync(kFull, eps_sq, l);
-      const float4 bbc = make_float4(__shfl_sync(kFull, bb_c.x, l), __shfl_sync(kFull, bb_c.y, l),
-                                     __shfl_sync(kFull, bb_c.z, l), __shfl_sync(kFull, bb_c.w, l));
-      const float4 bbn = make_float4(__shfl_sync(kFull, bb_n.x, l), __shfl_sync(kFull, bb_n.y, l),
-                                     __shfl_sync(kFull, bb_n.z, l), __shfl_sync(kFull, bb_n.w, l));
-      const int32_t a0 = __shfl_sync(kFull, c0, l), a1 = __shfl_sync(kFull, c1, l);
-      if (pair_scan(p, a0, a1, p.cell_start[nc], p.cell_start[nc + 1], bbc, bbn, e2) && lane == 0)
-        uf_unite(p.uf, cc, nc, d);
-      __syncwarp();
-    }
+    append(p.dlist, &d->d_count, deferred, t);
+  }
+}
+
+__global__ void __launch_bounds__(256) k_pair_warp(Plan p) {
+  Desc* d = p.desc;
+  const uint32_t nd = d->d_count;
+  const uint32_t lane = lane_id();
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < nd; w += nwarps) {
+    const int2 pr = p.plist[p.dlist[w]];
+    const int32_t c = pr.x, nb = pr.y;
+    const float eps_sq = p.seg_param[p.cell_seg[c]].eps_sq;
+    if (pair_scan(p, p.cell_start[c], p.cell_start[c + 1], p.cell_start[nb], p.cell_start[nb + 1],
+                  p.bbox[c], p.bbox[nb], eps_sq) && lane == 0)
+      uf_unite(p.uf, c, nb, d);
+    __syncwarp();
   }
 }
 
@@ -442,10 +477,19 @@ cudaError_t launch_core(const Plan& p, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+// Resets the pair lists between rings.
+__global__ void k_pairs_reset(Plan p) {
+  if (threadIdx.x == 0) { p.desc->p_count = 0; p.desc->d_count = 0; }
+}
+
 cudaError_t launch_union(const Plan& p, cudaStream_t s) {
-  k_union<<<p.num_sms * 8, kCellThreads, 0, s>>>(p, 0, 0);
-  k_flatten<<<p.num_sms * 8, 256, 0, s>>>(p);
-  k_union<<<p.num_sms * 8, kCellThreads, 0, s>>>(p, 1, 1);
+  for (int ring = 0; ring < 2; ++ring) {
+    if (ring == 1) k_flatten<<<p.num_sms * 8, 256, 0, s>>>(p);
+    k_pairs_reset<<<1, 32, 0, s>>>(p);
+    k_pairs<<<p.num_sms * 8, 256, 0, s>>>(p, ring, ring);
+    k_pair_scan<<<p.num_sms * 8, 256, 0, s>>>(p);
+    k_pair_warp<<<p.num_sms * 8, 256, 0, s>>>(p);
+  }
   return cudaGetLastError();
 }
 

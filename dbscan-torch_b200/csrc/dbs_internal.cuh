@@ -122,6 +122,8 @@ struct Desc {
   uint32_t dense_sort;  // 1: counting sort over the dense key space
   uint32_t q_count;     // core-query list length (points of cells below ms)
   uint32_t b_count;     // border list length (non-core points)
+  uint32_t p_count;     // union-find candidate pair list length
+  uint32_t d_count;     // pairs deferred to warp-cooperative scans
   uint32_t pad1;
   GridBar bar;
   // %globaltimer (ns) at each phase boundary of the cooperative kernels,
@@ -158,6 +160,9 @@ struct Plan {
   int32_t* cid;           // (n) cluster id per cell
   uint32_t* qlist;        // (n) sorted positions needing a core count
   uint32_t* blist;        // (n) sorted positions of non-core points
+  int2* plist;            // (pair_cap) candidate cell pairs (c, nc > c)
+  uint32_t* dlist;        // (pair_cap) indices into plist, over budget
+  int64_t pair_cap;       // entries available in plist / dlist
   int32_t* cell_map;      // dense cell map
   int64_t dense_cap;      // entries available in cell_map
   int32_t* big_cell;      // huge cells (> kHugeCell points): cell index

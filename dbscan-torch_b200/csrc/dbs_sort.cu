@@ -41,7 +41,7 @@ __global__ void k_init(Plan p) {
     d->big_packed = 0;
   }
   for (int64_t i = tid; i < 2 * kRadix; i += stride) (&d->digit_total[0][0])[i] = 0;
-  if (tid == 0) { d->bar.count = 0; d->bar.gen = 0; d->dense_sort = 0; d->q_count = 0; d->b_count = 0; }
+  if (tid == 0) { d->bar.count = 0; d->bar.gen = 0; d->dense_sort = 0; d->q_count = 0; d->b_count = 0; d->p_count = 0; d->d_count = 0; }
   for (int64_t i = tid; i < p.scan_tiles; i += stride) { p.rle_status[i] = 0; p.ids_status[i] = 0; }
   if (p.single && tid == 0) {
     p.seg_off[0] = 0;
