@@ -446,6 +446,9 @@ const char* dbs_strerror(int code) {
     case DBS_ERR_TOO_LARGE: return "too many points (n must be < 2^31)";
     case DBS_ERR_CUDA: return "CUDA runtime error";
     case DBS_ERR_DEVICE: return "device-side failure (bounded wait exceeded)";
+    case DBS_ERR_STATIC_LIMIT:
+      return "too many points for the built-in scratch (n must be <= DBS_STATIC_MAX_POINTS = 16384); "
+             "use dbs_dbscan2d with a workspace";
     default: return "unknown error";
   }
 }
@@ -460,3 +463,67 @@ const char* dbs_stage_name(int stage) {
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------ built-in scratch form
+// dbs_dbscan2d_static: the pipeline of dbs_dbscan2d on a workspace carved
+// out of a fixed array in this library's device image. Some callers have no
+// means to allocate device memory when they cluster -- a host plugin handed
+// device pointers but no allocator, an out-of-memory handler, a loop that
+// cannot afford the device-wide synchronisation of cudaMalloc / cudaFree --
+// so this form calls no allocating routine at all: the array is part of the
+// module image, its address is looked up once per device, and the launch
+// sequence is the one every other entry point runs.
+
+// The first kernel of every call (k_init) resets every counter, flag and
+// look-back word the later kernels read, so no byte has to start at zero.
+static __device__ __align__(256) unsigned char g_dbs_static_scratch[DBS_STATIC_SCRATCH_BYTES];
+
+namespace dbs {
+namespace {
+
+constexpr int kStaticDevices = 64;
+std::mutex g_static_mu;
+void* g_static_addr[kStaticDevices] = {nullptr};
+
+// Address of g_dbs_static_scratch on the current device. Set-up happens on
+// the first call made with that device current.
+int static_scratch(void** out) {
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kStaticDevices) return DBS_ERR_CUDA;
+  std::lock_guard<std::mutex> lock(g_static_mu);
+  if (g_static_addr[dev] == nullptr) {
+    void* a = nullptr;
+    if (cudaGetSymbolAddress(&a, g_dbs_static_scratch) != cudaSuccess || a == nullptr)
+      return DBS_ERR_CUDA;
+    g_static_addr[dev] = a;
+  }
+  *out = g_static_addr[dev];
+  return DBS_OK;
+}
+
+}  // namespace
+}  // namespace dbs
+
+extern "C" int dbs_dbscan2d_static(const float* X, int64_t n, double eps, int64_t min_samples,
+                                   int32_t* labels, uint32_t* status, void* stream) {
+  if (n < 0 || !(eps > 0.0) || min_samples < 1) return DBS_ERR_INVALID;
+  if (n > DBS_STATIC_MAX_POINTS) return DBS_ERR_STATIC_LIMIT;
+  if (n > 0 && (X == nullptr || labels == nullptr)) return DBS_ERR_INVALID;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (n == 0) {
+    if (status && cudaMemsetAsync(status, 0, sizeof(uint32_t), s) != cudaSuccess) return DBS_ERR_CUDA;
+    return DBS_OK;
+  }
+  void* ws = nullptr;
+  int rc = static_scratch(&ws);
+  if (rc != DBS_OK) return rc;
+  Plan p;
+  rc = prepare_single(X, n, eps, min_samples, labels, ws, DBS_STATIC_SCRATCH_BYTES, &p);
+  if (rc != DBS_OK) return rc;
+  rc = run_pipeline(p, s, nullptr);
+  if (rc != DBS_OK) return rc;
+  if (status && cudaMemcpyAsync(status, &p.desc->status, sizeof(uint32_t), cudaMemcpyDeviceToDevice,
+                                s) != cudaSuccess)
+    return DBS_ERR_CUDA;
+  return DBS_OK;
+}

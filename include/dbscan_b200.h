@@ -135,6 +135,46 @@ int dbs_read_plan(const void* ws, void* stream, int64_t* num_cells, int32_t* key
 const char* dbs_strerror(int code);
 const char* dbs_stage_name(int stage);
 
+/* ---------------------------------------------------------------------------
+ * Built-in scratch form. No counterpart in the reference: its extension
+ * always allocates through torch.
+ *
+ * dbs_dbscan2d_static runs the same pipeline as dbs_dbscan2d and returns the
+ * same labels, but takes no workspace and allocates nothing: its scratch is a
+ * fixed array of DBS_STATIC_SCRATCH_BYTES inside the library's device image,
+ * enough for clouds of up to DBS_STATIC_MAX_POINTS points. It serves callers
+ * that cannot allocate device memory when they cluster: a host plugin that is
+ * handed device pointers but no allocator, code running inside an
+ * out-of-memory handler or with the device memory already used up, and
+ * latency-bound loops that must not take the device-wide synchronisation of
+ * cudaMalloc / cudaFree.
+ *
+ *   - n > DBS_STATIC_MAX_POINTS is rejected with DBS_ERR_STATIC_LIMIT before
+ *     any CUDA call; use dbs_dbscan2d with a workspace for larger clouds.
+ *   - The first call made with a device current does the set-up for that
+ *     device: it looks up the address of the scratch array there
+ *     (cudaGetSymbolAddress, which may load the library's device code onto
+ *     the device). Make that first call before any stream capture begins.
+ *     The address is kept for the life of the process; after a
+ *     cudaDeviceReset of that device this entry point must not be used.
+ *   - Nothing in the scratch has to start at zero: the first kernel of every
+ *     call resets each counter, flag and look-back word the later kernels
+ *     read.
+ *   - All calls on one device share the one array. Calls whose work overlaps
+ *     on the device race on it and return wrong labels: issue them on one
+ *     stream, or order them (events, synchronisation) across streams and
+ *     host threads. Calls on different devices do not interact.
+ *   - status (nullable, device memory) receives the call's device status
+ *     word (0, or DBS_STATUS_* bits) by a stream-ordered copy.
+ *   - n == 0 is a no-op (a non-NULL status is set to 0).
+ */
+#define DBS_STATIC_MAX_POINTS 16384
+#define DBS_STATIC_SCRATCH_BYTES (8u << 20)
+#define DBS_ERR_STATIC_LIMIT 6  /* n > DBS_STATIC_MAX_POINTS (dbs_dbscan2d_static) */
+
+int dbs_dbscan2d_static(const float* X, int64_t n, double eps, int64_t min_samples,
+                        int32_t* labels, uint32_t* status, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
