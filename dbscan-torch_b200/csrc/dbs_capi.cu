@@ -427,14 +427,14 @@ int dbs_read_plan(const void* ws, void* stream, int64_t* num_cells, int32_t* key
   if (ws == nullptr) return DBS_ERR_INVALID;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const Desc* d = static_cast<const Desc*>(ws);
-  uint32_t head[6] = {0, 0, 0, 0, 0, 0};  // status, key64, nbits, npasses, num_cells, pad
-  if (cudaMemcpyAsync(head, d, sizeof(head), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+  Desc h;
+  if (cudaMemcpyAsync(&h, d, sizeof(Desc), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
       cudaStreamSynchronize(s) != cudaSuccess)
     return DBS_ERR_CUDA;
-  if (num_cells) *num_cells = head[4];
-  if (key_bits) *key_bits = (int32_t)head[2];
-  if (passes) *passes = (int32_t)head[3];
-  if (key_bytes) *key_bytes = head[1] ? 8 : 4;
+  if (num_cells) *num_cells = h.num_cells;
+  if (key_bits) *key_bits = (int32_t)h.nbits;
+  if (passes) *passes = h.dense_sort ? 0 : (int32_t)h.npasses;
+  if (key_bytes) *key_bytes = h.key64 ? 8 : 4;
   return DBS_OK;
 }
 

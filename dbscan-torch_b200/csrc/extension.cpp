@@ -163,6 +163,33 @@ torch::Tensor run_cuda(const torch::Tensor& Xc, double eps, int64_t min_samples)
   return labels;
 }
 
+// A CPU tensor in, CPU labels out, through the host-buffer entry point: one
+// copy in (asynchronous when X is pinned), the pipeline, one copy out into a
+// pinned tensor from the caching host allocator, then a stream synchronise.
+torch::Tensor run_host(const torch::Tensor& Xh, double eps, int64_t min_samples) {
+  TORCH_CHECK(torch::cuda::is_available(),
+              "dbscan_torch (B200 build) runs on a CUDA device only and none is available; "
+              "there is no CPU implementation in this build");
+  const torch::Device dev(torch::kCUDA, c10::cuda::current_device());
+  c10::cuda::CUDAGuard guard(dev);
+  const int64_t n = Xh.size(0);
+  auto labels = torch::empty({n}, torch::TensorOptions().dtype(torch::kInt32).pinned_memory(true));
+  cudaStream_t stream = at::cuda::getCurrentCUDAStream();
+  if (!capturing(stream)) drain(false);
+  const size_t bytes = dbs_host_workspace_bytes(n);
+  auto ws = alloc_ws(bytes, dev);
+  const int rc = dbs_dbscan2d_host(Xh.data_ptr<float>(), n, eps, min_samples,
+                                   labels.data_ptr<int32_t>(), ws.data_ptr(), bytes, stream);
+  if (rc == DBS_ERR_DEVICE) {
+    uint32_t st = 0;
+    check_rc(dbs_read_status(ws.data_ptr(), stream, &st), "dbscan2d");
+    TORCH_CHECK(false, "dbscan2d: device-side failure (status 0x", std::hex, st, std::dec,
+                "): a bounded wait in the pipeline ran out");
+  }
+  check_rc(rc, "dbscan2d");
+  return labels;
+}
+
 }  // namespace
 
 torch::Tensor dbscan2d(torch::Tensor X, double eps, int64_t min_samples) {
@@ -170,9 +197,7 @@ torch::Tensor dbscan2d(torch::Tensor X, double eps, int64_t min_samples) {
   if (X.is_cuda()) return run_cuda(X.contiguous(), eps, min_samples);
   if (X.size(0) == 0)
     return torch::empty({0}, torch::TensorOptions().dtype(torch::kInt32));
-  auto Xd = require_cuda_copy(X.contiguous());
-  auto labels = run_cuda(Xd, eps, min_samples);
-  return labels.to(torch::kCPU);
+  return run_host(X.contiguous(), eps, min_samples);
 }
 
 std::pair<torch::Tensor, std::map<std::string, float>> dbscan2d_profile(torch::Tensor X, double eps,

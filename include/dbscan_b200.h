@@ -127,7 +127,8 @@ int dbs_read_status(const void* ws, void* stream, uint32_t* status);
 
 /* Shape of the last call on this workspace, read after synchronising the
  * stream: number of cells (distinct occupied grid cells over all clouds),
- * significant bits of the compacted cell keys, radix passes that ran, and
+ * significant bits of the compacted cell keys, radix passes that ran (0 when
+ * every cloud fit the dense key space and the counting sort ran instead), and
  * bytes per stored key (4 or 8). Any output pointer may be NULL. */
 int dbs_read_plan(const void* ws, void* stream, int64_t* num_cells, int32_t* key_bits,
                   int32_t* passes, int32_t* key_bytes);
