@@ -12,9 +12,11 @@
 // also record each cell in a dense map indexed by the compacted key, so
 // neighbour lookup is one load instead of a binary search.
 //
-// k_cell_prep gives each cell one thread: it folds the bounding box of the
+// k_cell_prep gives each cell one lane: it folds the bounding box of the
 // cell's points and resolves the 25 offsets of the 5x5 stencil in the
-// reference's order (off = (dx+2)*5 + (dy+2)).
+// reference's order (off = (dx+2)*5 + (dy+2)); the warp then walks its cells'
+// contiguous points to record each point's cell and class (core wholesale,
+// or a query for k_core; k_core_pass1 :199-208).
 #include "dbs_internal.cuh"
 
 namespace dbs {
@@ -138,35 +140,52 @@ __device__ __forceinline__ int32_t find_cell(const Plan& p, const SegInfo& g, in
 
 constexpr int32_t kBigCell = 64;  // cells above this size reduce their box per warp
 
-// One thread per cell: bounding box of the cell's points and the 25-entry
-// neighbour row. Cells larger than kBigCell points get their box from the
-// whole warp afterwards (a 2M-point cell would otherwise be one thread's
-// serial loop).
+// Warp-aggregated append of the lanes with `take` to a work list.
+__device__ __forceinline__ void append_list(uint32_t* list, uint32_t* count, bool take, uint32_t v) {
+  const uint32_t m = __ballot_sync(0xffffffffu, take);
+  if (m == 0) return;
+  uint32_t base = 0;
+  if (lane_id() == 0) base = atomicAdd(count, (uint32_t)__popc(m));
+  base = __shfl_sync(0xffffffffu, base, 0);
+  if (take) list[base + __popc(m & lanemask_lt())] = v;
+}
+
+// One warp per 32 consecutive cells (lane = cell):
+//   - bounding box of each cell's points (cells above kBigCell points get
+//     theirs from the whole warp; cells above kHugeCell from k_huge_bbox);
+//   - the warp's cells own one contiguous range of sorted points: each point
+//     gets its cell, and its class (k_core_pass1, dbscan_cuda.cu:199-208): a
+//     point of a cell with >= ms points is core wholesale, any other point
+//     goes to the query list of k_core. Point-parallel, so the stores are
+//     coalesced;
+//   - the 25-entry neighbour row of each cell, staged in shared memory and
+//     written as one contiguous block per warp.
 __global__ void __launch_bounds__(kCellThreads) k_cell_prep(Plan p) {
+  __shared__ int32_t s_row[kCellThreads / 32][32 * kNgh];
   const uint32_t full = 0xffffffffu;
   const uint32_t lane = lane_id();
+  int32_t* srow = s_row[threadIdx.x >> 5];
   const uint32_t C = p.desc->num_cells;
   const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
   for (uint32_t wbase = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; wbase < C;
        wbase += warps * 32) {
     const uint32_t c = wbase + lane;
     const bool valid = c < C;
-    int32_t s0 = 0, s1 = 0;
-    if (valid) { s0 = p.cell_start[c]; s1 = p.cell_start[c + 1]; }
+    int32_t s0 = INT32_MAX, s1 = INT32_MAX, seg = 0;
+    if (valid) { s0 = p.cell_start[c]; s1 = p.cell_start[c + 1]; seg = p.cell_seg[c]; }
     const bool big = valid && (s1 - s0) > kBigCell;
+    const bool huge = big && (s1 - s0) > kHugeCell;
+    const bool dense = valid && (s1 - s0) >= p.seg_param[seg].ms;
     if (valid && !big) {
-      // Gather the cell's sorted coordinates (the reference's k_gather_xy),
-      // record each point's cell, fold the box. A one-point cell keeps its
-      // raw coordinates: the reference seeds the fold with xs[s] and flushes
-      // subnormals only through fminf/fmaxf.
+      // Fold the box. A one-point cell keeps its raw coordinates: the
+      // reference seeds the fold with xs[s] and flushes subnormals only
+      // through fminf/fmaxf.
       float2 v = p.xy[s0];
-      p.point_cell[s0] = (int32_t)c;
       float4 b = make_float4(v.x, v.x, v.y, v.y);
       if (s1 - s0 > 1) {
         b = make_float4(fminf(v.x, INFINITY), fmaxf(v.x, -INFINITY), fminf(v.y, INFINITY),
                         fmaxf(v.y, -INFINITY));
         for (int32_t i = s0 + 1; i < s1; ++i) {
-          p.point_cell[i] = (int32_t)c;
           v = p.xy[i];
           b.x = fminf(b.x, v.x); b.y = fmaxf(b.y, v.x);
           b.z = fminf(b.z, v.y); b.w = fmaxf(b.w, v.y);
@@ -174,7 +193,6 @@ __global__ void __launch_bounds__(kCellThreads) k_cell_prep(Plan p) {
       }
       p.bbox[c] = b;
     }
-    const bool huge = big && (s1 - s0) > kHugeCell;
     if (huge) {
       // Registered for k_huge_bbox: one entry, ceil(size / kHugeChunk) chunks.
       const unsigned long long nch = (unsigned long long)((s1 - s0 + kHugeChunk - 1) / kHugeChunk);
@@ -191,10 +209,8 @@ __global__ void __launch_bounds__(kCellThreads) k_cell_prep(Plan p) {
       const int l = __ffs(bm) - 1;
       bm &= bm - 1;
       const int32_t b0 = __shfl_sync(full, s0, l), b1 = __shfl_sync(full, s1, l);
-      const int32_t cl = (int32_t)__shfl_sync(full, c, l);
       float xmin = INFINITY, xmax = -INFINITY, ymin = INFINITY, ymax = -INFINITY;
       for (int32_t i = b0 + lane; i < b1; i += 32) {
-        p.point_cell[i] = cl;
         const float2 v = p.xy[i];
         xmin = fminf(xmin, v.x); xmax = fmaxf(xmax, v.x);
         ymin = fminf(ymin, v.y); ymax = fmaxf(ymax, v.y);
@@ -208,30 +224,63 @@ __global__ void __launch_bounds__(kCellThreads) k_cell_prep(Plan p) {
       }
       if ((int)lane == l) p.bbox[c] = make_float4(xmin, xmax, ymin, ymax);
     }
-    if (!valid) continue;
-    // Neighbour row, off = (dx+2)*5 + (dy+2) as in the reference.
-    const int32_t s = p.cell_seg[c];
-    const SegInfo& g = p.seg_info[s];
-    const uint64_t local = p.cell_key[c] - g.base;
-    const uint64_t gx = local >> g.ysh;
-    const uint64_t gy = local & ((1ull << g.ysh) - 1ull);
-    const int32_t kx = expand_axis(gx, g.bx, g.px);
-    const int32_t ky = expand_axis(gy, g.by, g.py);
-    uint64_t ngy[5];
+
+    // Points of the warp's cells, runs of consecutive non-huge cells at a
+    // time (huge cells' points are classified by k_huge_bbox).
+    uint32_t todo = __ballot_sync(full, valid && !huge);
+    while (todo) {
+      const int la = __ffs(todo) - 1;
+      const uint32_t run = todo >> la;
+      const int len = (~run) ? __ffs(~run) - 1 : 32 - la;
+      todo &= ~((len >= 32 ? full : ((1u << len) - 1u)) << la);
+      const int32_t a = __shfl_sync(full, s0, la), b = __shfl_sync(full, s1, la + len - 1);
+      for (int32_t base = a; base < b; base += 32) {
+        const int32_t i = base + (int32_t)lane;
+        const bool ok = i < b;
+        // Lane (cell) of point i: the last lane whose first point is <= i.
+        int lo = 0;
 #pragma unroll
-    for (int dy = 0; dy < 5; ++dy)
-      ngy[dy] = compact_axis((int32_t)((uint32_t)ky + (uint32_t)(dy - 2)), g.by, g.py);
-    int32_t* row = p.ngh + (int64_t)c * kNgh;
-#pragma unroll
-    for (int dx = 0; dx < 5; ++dx) {
-      const uint64_t ngx = compact_axis((int32_t)((uint32_t)kx + (uint32_t)(dx - 2)), g.bx, g.px);
-#pragma unroll
-      for (int dy = 0; dy < 5; ++dy) {
-        int32_t r = -1;
-        if (ngx != ~0ull && ngy[dy] != ~0ull) r = find_cell(p, g, s, ngx, ngy[dy], C);
-        row[dx * 5 + dy] = r;
+        for (int step = 16; step > 0; step >>= 1) {
+          const int32_t sp = __shfl_sync(full, s0, lo + step);
+          if (sp <= i) lo += step;
+        }
+        const bool dn = __shfl_sync(full, dense, lo);
+        if (ok) {
+          p.point_cell[i] = (int32_t)(wbase + lo);
+          p.is_core[i] = dn ? 1 : 0;
+        }
+        append_list(p.qlist, &p.desc->q_count, ok && !dn, (uint32_t)i);
       }
     }
+
+    // Neighbour row, off = (dx+2)*5 + (dy+2) as in the reference.
+    if (valid) {
+      const SegInfo& g = p.seg_info[seg];
+      const uint64_t local = p.cell_key[c] - g.base;
+      const uint64_t gx = local >> g.ysh;
+      const uint64_t gy = local & ((1ull << g.ysh) - 1ull);
+      const int32_t kx = expand_axis(gx, g.bx, g.px);
+      const int32_t ky = expand_axis(gy, g.by, g.py);
+      uint64_t ngy[5];
+#pragma unroll
+      for (int dy = 0; dy < 5; ++dy)
+        ngy[dy] = compact_axis((int32_t)((uint32_t)ky + (uint32_t)(dy - 2)), g.by, g.py);
+#pragma unroll
+      for (int dx = 0; dx < 5; ++dx) {
+        const uint64_t ngx = compact_axis((int32_t)((uint32_t)kx + (uint32_t)(dx - 2)), g.bx, g.px);
+#pragma unroll
+        for (int dy = 0; dy < 5; ++dy) {
+          int32_t r = -1;
+          if (ngx != ~0ull && ngy[dy] != ~0ull) r = find_cell(p, g, seg, ngx, ngy[dy], C);
+          srow[lane * kNgh + dx * 5 + dy] = r;
+        }
+      }
+    }
+    __syncwarp();
+    const int32_t rows = (int32_t)min(32u, C - wbase);
+    int32_t* out = p.ngh + (int64_t)wbase * kNgh;
+    for (int32_t k = (int32_t)lane; k < rows * kNgh; k += 32) out[k] = srow[k];
+    __syncwarp();
   }
 }
 
@@ -264,11 +313,20 @@ __global__ void __launch_bounds__(256) k_huge_bbox(Plan p) {
     const int32_t k = (int32_t)(g - p.big_base[lo]);
     const int32_t a = s0 + k * kHugeChunk, b = min(s1, a + kHugeChunk);
     float xmin = INFINITY, xmax = -INFINITY, ymin = INFINITY, ymax = -INFINITY;
-    for (int32_t i = a + lane; i < b; i += 32) {
-      p.point_cell[i] = c;
-      const float2 v = p.xy[i];
-      xmin = fminf(xmin, v.x); xmax = fmaxf(xmax, v.x);
-      ymin = fminf(ymin, v.y); ymax = fmaxf(ymax, v.y);
+    // The chunk's points also get their cell and class, as k_cell_prep gives
+    // every other point (a huge cell is below ms only when ms > kHugeCell).
+    const bool dn = (s1 - s0) >= p.seg_param[p.cell_seg[c]].ms;
+    for (int32_t base = a; base < b; base += 32) {
+      const int32_t i = base + (int32_t)lane;
+      const bool ok = i < b;
+      if (ok) {
+        p.point_cell[i] = c;
+        p.is_core[i] = dn ? 1 : 0;
+        const float2 v = p.xy[i];
+        xmin = fminf(xmin, v.x); xmax = fmaxf(xmax, v.x);
+        ymin = fminf(ymin, v.y); ymax = fmaxf(ymax, v.y);
+      }
+      append_list(p.qlist, &d->q_count, ok && !dn, (uint32_t)i);
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {

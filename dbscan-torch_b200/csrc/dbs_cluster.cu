@@ -32,25 +32,6 @@ __device__ __forceinline__ void append(uint32_t* list, uint32_t* count, bool tak
   if (take) list[base + __popc(m & lanemask_lt())] = v;
 }
 
-// Point classification, one thread per sorted point: a point of a cell with
-// >= ms points is core wholesale (k_core_pass1, dbscan_cuda.cu:199-208);
-// every other point goes to the query list of k_core, so that k_core's warps
-// hold only points with a neighbour scan to do.
-__global__ void __launch_bounds__(256) k_classify(Plan p) {
-  const int64_t n = p.n;
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < n; base += stride) {
-    const int64_t i = base + threadIdx.x;
-    bool query = false;
-    if (i < n) {
-      const int32_t c = p.point_cell[i];
-      if (p.cell_start[c + 1] - p.cell_start[c] >= p.seg_param[p.cell_seg[c]].ms) p.is_core[i] = 1;
-      else query = true;
-    }
-    append(p.qlist, &p.desc->q_count, query, (uint32_t)i);
-  }
-}
-
 // Core flag of every query point, one thread per query. A query counts its
 // own cell wholesale (the reference never distance-tests the centre cell,
 // :231-233) plus the points within eps of the other 24 stencil cells that
@@ -471,7 +452,6 @@ __global__ void __launch_bounds__(kCellThreads) k_labels(Plan p) {
 
 // ------------------------------------------------------------- launchers
 cudaError_t launch_core(const Plan& p, cudaStream_t s) {
-  k_classify<<<p.num_sms * 8, 256, 0, s>>>(p);
   k_core<<<p.num_sms * 8, kCellThreads, 0, s>>>(p);
   k_status<<<p.num_sms * 8, 256, 0, s>>>(p);
   return cudaGetLastError();

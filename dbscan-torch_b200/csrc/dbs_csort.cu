@@ -33,14 +33,30 @@ namespace dbs {
 constexpr int kCsThreads = 256;
 constexpr uint32_t kFullMask = 0xffffffffu;
 
-// Global key of point v of cloud seg (dense mode: fits 31 bits).
-__device__ __forceinline__ uint32_t dense_key(const Plan& p, float2 v, int32_t seg) {
-  const SegInfo& g = p.seg_info[seg];
-  const float inv_r = p.seg_param[seg].inv_r;
-  const uint64_t gx = compact_axis(cell_coord(v.x, inv_r), g.bx, g.px);
-  const uint64_t gy = compact_axis(cell_coord(v.y, inv_r), g.by, g.py);
-  return (uint32_t)(g.base + (gx << g.ysh) + gy);
-}
+// Per-cloud scalars of the dense key of a point (its dense-map index, which
+// fits 31 bits), held in registers while a thread's points stay in one cloud.
+struct KeyCtx {
+  int32_t bx[4], by[4];
+  uint64_t px, py, base;
+  uint32_t ysh;
+  float inv_r;
+  int64_t end;  // first input index past the cloud
+  int32_t seg;
+  __device__ void load(const Plan& p, int32_t s) {
+    const SegInfo& g = p.seg_info[s];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) { bx[k] = g.bx[k]; by[k] = g.by[k]; }
+    px = g.px; py = g.py; base = g.base; ysh = g.ysh;
+    inv_r = p.seg_param[s].inv_r;
+    end = p.seg_off[s + 1];
+    seg = s;
+  }
+  __device__ uint32_t key(float2 v) const {
+    const uint64_t gx = compact_axis(cell_coord(v.x, inv_r), bx, px);
+    const uint64_t gy = compact_axis(cell_coord(v.y, inv_r), by, py);
+    return (uint32_t)(base + (gx << ysh) + gy);
+  }
+};
 
 // Points per lane and iteration of the point loops: independent loads and
 // atomics in flight per thread.
@@ -113,54 +129,21 @@ __device__ __forceinline__ void block_scan2(uint32_t a, uint32_t b, uint32_t& xa
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(kCsThreads) k_csort(Plan p) {
-  __shared__ uint32_t s_a[kCsThreads / 32], s_b[kCsThreads / 32];
+// Exclusive scan of the per-key counts bins[0, W) of the dense key space
+// (per-block range sums, a scan of the block sums by block 0, a rescan).
+// Afterwards bins[b] is key b's first sorted position, and the cells exist:
+// cell_map (key -> cell or -1), cell_start / cell_key / cell_seg, each
+// cloud's cell_begin and num_cells. Cells are numbered in ascending key
+// order, as the reference's run-length pass over sorted keys numbers them.
+// Ends with a grid barrier.
+__device__ __forceinline__ void scan_bins(const Plan& p, int64_t W, uint32_t* s_a, uint32_t* s_b) {
   Desc* d = p.desc;
-  if (!d->dense_sort) return;
   const int64_t n = p.n;
-  const int64_t W = (int64_t)d->dense_total;
   uint32_t* bins = p.bin_count;
-  const uint32_t lane = lane_id();
-  const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int64_t nthr = (int64_t)gridDim.x * blockDim.x;
-
-  // 0. clear counters
-  mark_phase(d, 0);
-  for (int64_t b = tid; b < W; b += nthr) bins[b] = 0;
-  grid_sync(&d->bar, d);
-  mark_phase(d, 1);
-
-  // 1. count. Each warp takes kU consecutive 32-point rows per iteration;
-  // peers = lanes with the same key, one atomic per peer group.
-  const int64_t gwarp = tid >> 5, nwarps = nthr >> 5;
-  {
-    int32_t seg = seg_of(p, min(gwarp * 32 * kU + lane, n > 0 ? n - 1 : 0));
-    for (int64_t base = gwarp * 32 * kU; base < n; base += nwarps * 32 * kU) {
-      float2 v[kU];
-#pragma unroll
-      for (int k = 0; k < kU; ++k) {
-        const int64_t i = base + k * 32 + lane;
-        v[k] = i < n ? p.X[i] : make_float2(0.f, 0.f);
-      }
-#pragma unroll
-      for (int k = 0; k < kU; ++k) {
-        const int64_t i = base + k * 32 + lane;
-        const bool valid = i < n;
-        uint32_t key = 0xffffffffu;
-        if (valid) {
-          while (i >= p.seg_off[seg + 1]) ++seg;
-          key = dense_key(p, v[k], seg);
-        }
-        const Agg a = aggregate(key, valid);
-        if (valid && lane == a.leader) atomicAdd(&bins[key], (uint32_t)__popc(a.group));
-      }
-    }
-  }
-  grid_sync(&d->bar, d);
-  mark_phase(d, 2);
-
-  // 2. block range sums
-  const int64_t per = (W + gridDim.x - 1) / gridDim.x;
+  constexpr int kI = 8;  // consecutive keys per thread in the rescan
+  // Ranges of whole 8-key groups (16-byte aligned: bins and cell_map start
+  // on 256-byte boundaries).
+  const int64_t per = (((W + gridDim.x - 1) / gridDim.x) + kI - 1) & ~(int64_t)(kI - 1);
   const int64_t r0 = min(W, (int64_t)blockIdx.x * per), r1 = min(W, r0 + per);
   {
     uint32_t cs = 0, ne = 0;
@@ -174,9 +157,8 @@ __global__ void __launch_bounds__(kCsThreads) k_csort(Plan p) {
     if (threadIdx.x == 0) { p.blk_sum[blockIdx.x] = ta; p.blk_ne[blockIdx.x] = tb; }
   }
   grid_sync(&d->bar, d);
-  mark_phase(d, 3);
 
-  // 3. exclusive scan of block sums (block 0; gridDim.x <= kMaxGrid)
+  // Exclusive scan of block sums (block 0; gridDim.x <= kMaxGrid).
   if (blockIdx.x == 0) {
     const int per_t = (gridDim.x + blockDim.x - 1) / blockDim.x;
     const int a0 = threadIdx.x * per_t, a1 = min((int)gridDim.x, a0 + per_t);
@@ -197,41 +179,124 @@ __global__ void __launch_bounds__(kCsThreads) k_csort(Plan p) {
     }
   }
   grid_sync(&d->bar, d);
-  mark_phase(d, 4);
 
-  // 4. rescan: offsets, dense cell map, cells
+  // Rescan: eight consecutive keys per thread (16-byte loads and stores),
+  // one block scan per 8 * blockDim.x keys.
   {
+    const bool one = p.nseg == 1;
+    const uint64_t base0 = p.seg_info[0].base;
     uint32_t carry_cs = p.blk_sum[blockIdx.x], carry_ne = p.blk_ne[blockIdx.x];
-    for (int64_t cb = r0; cb < r1; cb += blockDim.x) {
-      const int64_t b = cb + threadIdx.x;
-      const uint32_t c = b < r1 ? bins[b] : 0u;
-      const uint32_t f = c != 0;
+    for (int64_t cb = r0; cb < r1; cb += (int64_t)blockDim.x * kI) {
+      const int64_t b0 = cb + (int64_t)threadIdx.x * kI;
+      const bool full = b0 + kI <= r1;
+      uint32_t c[kI];
+      if (full) {
+        const uint4 lo = *reinterpret_cast<const uint4*>(bins + b0);
+        const uint4 hi = *reinterpret_cast<const uint4*>(bins + b0 + 4);
+        c[0] = lo.x; c[1] = lo.y; c[2] = lo.z; c[3] = lo.w;
+        c[4] = hi.x; c[5] = hi.y; c[6] = hi.z; c[7] = hi.w;
+      } else {
+#pragma unroll
+        for (int k = 0; k < kI; ++k) c[k] = b0 + k < r1 ? bins[b0 + k] : 0u;
+      }
+      uint32_t cs = 0, ne = 0;
+#pragma unroll
+      for (int k = 0; k < kI; ++k) { cs += c[k]; ne += c[k] != 0; }
       uint32_t xa, xb, ta, tb;
-      block_scan2(c, f, xa, xb, ta, tb, s_a, s_b);
-      if (b < r1) {
-        const uint32_t off = carry_cs + xa;
-        const uint32_t cell = carry_ne + xb;
-        bins[b] = off;
-        p.cell_map[b] = f ? (int32_t)cell : -1;
-        const int32_t sg = seg_of_key(p, (uint64_t)b);
-        if ((uint64_t)b == p.seg_info[sg].base) p.seg_info[sg].cell_begin = (int32_t)cell;
-        if (f) {
-          p.cell_start[cell] = (int32_t)off;
-          p.cell_key[cell] = (uint64_t)b;
-          p.cell_seg[cell] = sg;
+      block_scan2(cs, ne, xa, xb, ta, tb, s_a, s_b);
+      uint32_t off = carry_cs + xa, cell = carry_ne + xb;
+      uint32_t o[kI];
+      int32_t m[kI];
+#pragma unroll
+      for (int k = 0; k < kI; ++k) {
+        const int64_t b = b0 + k;
+        o[k] = off;
+        m[k] = c[k] ? (int32_t)cell : -1;
+        if (b < r1) {
+          const int32_t sg = one ? 0 : seg_of_key(p, (uint64_t)b);
+          if ((uint64_t)b == (one ? base0 : p.seg_info[sg].base)) p.seg_info[sg].cell_begin = (int32_t)cell;
+          if (c[k]) {
+            p.cell_start[cell] = (int32_t)off;
+            p.cell_key[cell] = (uint64_t)b;
+            p.cell_seg[cell] = sg;
+          }
         }
+        off += c[k];
+        cell += c[k] != 0;
+      }
+      if (full) {
+        *reinterpret_cast<uint4*>(bins + b0) = make_uint4(o[0], o[1], o[2], o[3]);
+        *reinterpret_cast<uint4*>(bins + b0 + 4) = make_uint4(o[4], o[5], o[6], o[7]);
+        *reinterpret_cast<int4*>(p.cell_map + b0) = make_int4(m[0], m[1], m[2], m[3]);
+        *reinterpret_cast<int4*>(p.cell_map + b0 + 4) = make_int4(m[4], m[5], m[6], m[7]);
+      } else {
+#pragma unroll
+        for (int k = 0; k < kI; ++k)
+          if (b0 + k < r1) { bins[b0 + k] = o[k]; p.cell_map[b0 + k] = m[k]; }
       }
       carry_cs += ta;
       carry_ne += tb;
     }
   }
   grid_sync(&d->bar, d);
-  mark_phase(d, 5);
+}
 
-  // 5. scatter
+__global__ void __launch_bounds__(kCsThreads, 5) k_csort(Plan p) {
+  __shared__ uint32_t s_a[kCsThreads / 32], s_b[kCsThreads / 32];
+  Desc* d = p.desc;
+  if (!d->dense_sort) return;
+  const int64_t n = p.n;
+  const int64_t W = (int64_t)d->dense_total;
+  uint32_t* bins = p.bin_count;
+  const uint32_t lane = lane_id();
+  const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t nthr = (int64_t)gridDim.x * blockDim.x;
+
+  // 0. clear counters
+  mark_phase(d, 0);
+  for (int64_t b = tid; b < W; b += nthr) bins[b] = 0;
+  grid_sync(&d->bar, d);
+  mark_phase(d, 1);
+
+  // 1. count. Each warp takes kU consecutive 32-point rows per iteration;
+  // peers = lanes with the same key, one atomic per peer group.
+  const int64_t gwarp = tid >> 5, nwarps = nthr >> 5;
+  {
+    KeyCtx kc;
+    kc.load(p, seg_of(p, min(gwarp * 32 * kU + lane, n > 0 ? n - 1 : 0)));
+    for (int64_t base = gwarp * 32 * kU; base < n; base += nwarps * 32 * kU) {
+      float2 v[kU];
+#pragma unroll
+      for (int k = 0; k < kU; ++k) {
+        const int64_t i = base + k * 32 + lane;
+        v[k] = i < n ? p.X[i] : make_float2(0.f, 0.f);
+      }
+#pragma unroll
+      for (int k = 0; k < kU; ++k) {
+        const int64_t i = base + k * 32 + lane;
+        const bool valid = i < n;
+        uint32_t key = 0xffffffffu;
+        if (valid) {
+          while (i >= kc.end) kc.load(p, kc.seg + 1);
+          key = kc.key(v[k]);
+        }
+        const Agg a = aggregate(key, valid);
+        if (valid && lane == a.leader) atomicAdd(&bins[key], (uint32_t)__popc(a.group));
+      }
+    }
+  }
+  grid_sync(&d->bar, d);
+  mark_phase(d, 2);
+
+  scan_bins(p, W, s_a, s_b);
+  mark_phase(d, 3);
+
+  // 5. scatter every point's input index to the slot its key's fetch-add
+  //    returns (perm)
   {
     const uint32_t lt = lanemask_lt();
-    int32_t seg = seg_of(p, min(gwarp * 32 * kU + lane, n > 0 ? n - 1 : 0));
+    KeyCtx kc;
+    kc.load(p, seg_of(p, min(gwarp * 32 * kU + lane, n > 0 ? n - 1 : 0)));
     for (int64_t base = gwarp * 32 * kU; base < n; base += nwarps * 32 * kU) {
       float2 v[kU];
 #pragma unroll
@@ -246,8 +311,8 @@ __global__ void __launch_bounds__(kCsThreads) k_csort(Plan p) {
         const int64_t i = base + k * 32 + lane;
         uint32_t key = 0xffffffffu;
         if (i < n) {
-          while (i >= p.seg_off[seg + 1]) ++seg;
-          key = dense_key(p, v[k], seg);
+          while (i >= kc.end) kc.load(p, kc.seg + 1);
+          key = kc.key(v[k]);
         }
         ag[k] = aggregate(key, i < n);
         pos[k] = 0;
@@ -262,10 +327,12 @@ __global__ void __launch_bounds__(kCsThreads) k_csort(Plan p) {
     }
   }
   grid_sync(&d->bar, d);
-  mark_phase(d, 6);
+  mark_phase(d, 4);
 
   // 6. gather the sorted coordinates (the reference's k_gather_xy):
   //    coalesced perm reads and xy writes, independent random reads of X.
+  //    (Writing the coordinates in the scatter instead costs more: random
+  //    8-byte writes leave partial sectors.)
   for (int64_t i0 = tid; i0 < n; i0 += nthr * kU) {
     uint32_t src[kU];
 #pragma unroll
@@ -280,7 +347,7 @@ __global__ void __launch_bounds__(kCsThreads) k_csort(Plan p) {
     }
   }
   __syncthreads();
-  mark_phase(d, 7);
+  mark_phase(d, 5);
 }
 
 cudaError_t launch_csort(const Plan& p, cudaStream_t s) {

@@ -94,6 +94,47 @@ __global__ void __launch_bounds__(256) k_bounds(Plan p) {
   float inv_r = p.seg_param[seg].inv_r;
   AxisAcc ax, ay;
   ax.reset(); ay.reset();
+  if (b1 <= seg_end) {
+    // The whole chunk lies in one cloud (every chunk of a plain call): four
+    // independent loads per thread in flight, then one flush per block.
+    __shared__ int32_t s_b[8];
+    if (threadIdx.x < 8) {  // lo_pos, hi_pos, lo_neg, hi_neg of x, then of y (AxisAcc::reset)
+      const int32_t r = threadIdx.x & 3;
+      s_b[threadIdx.x] = r == 0 ? INT32_MAX : r == 1 ? -1 : r == 2 ? 0 : INT32_MIN;
+    }
+    constexpr int kB = 4;
+    int64_t base = b0;
+    for (; base + kB * (int64_t)blockDim.x <= b1; base += kB * (int64_t)blockDim.x) {
+      float2 v[kB];
+#pragma unroll
+      for (int k = 0; k < kB; ++k) v[k] = p.X[base + k * (int64_t)blockDim.x + threadIdx.x];
+#pragma unroll
+      for (int k = 0; k < kB; ++k) {
+        ax.add(cell_coord(v[k].x, inv_r));
+        ay.add(cell_coord(v[k].y, inv_r));
+      }
+    }
+    for (int64_t i = base + threadIdx.x; i < b1; i += blockDim.x) {
+      const float2 v = p.X[i];
+      ax.add(cell_coord(v.x, inv_r));
+      ay.add(cell_coord(v.y, inv_r));
+    }
+    warp_fold(ax); warp_fold(ay);
+    __syncthreads();
+    if (lane_id() == 0) {
+      atomicMin(&s_b[0], ax.lo_pos); atomicMax(&s_b[1], ax.hi_pos);
+      atomicMin(&s_b[2], ax.lo_neg); atomicMax(&s_b[3], ax.hi_neg);
+      atomicMin(&s_b[4], ay.lo_pos); atomicMax(&s_b[5], ay.hi_pos);
+      atomicMin(&s_b[6], ay.lo_neg); atomicMax(&s_b[7], ay.hi_neg);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      AxisAcc bx{s_b[0], s_b[1], s_b[2], s_b[3]}, by{s_b[4], s_b[5], s_b[6], s_b[7]};
+      bx.flush(p.seg_info[seg].bx);
+      by.flush(p.seg_info[seg].by);
+    }
+    return;
+  }
   for (int64_t base = b0; base < b1; base += blockDim.x) {
     const int64_t i = base + threadIdx.x;
     // The cloud of the whole block-row: when the row is inside one cloud

@@ -1,0 +1,74 @@
+"""The sort step on key spaces of every size class, against the oracle
+(bit-exact labels).
+
+Points sit in W = wx * 2^ceil(log2 wy) compacted cell keys (cell side
+eps / sqrt(2)). A dense key space (W <= 4N + 4096) takes the counting sort
+over keys, whose per-key counters, scan and dense cell map all scale with W;
+a sparse one takes the radix sort. The clouds below cover W from under a
+million keys to 18 million, a sparse key space, a cloud with most points in
+a few cells, and many dense clouds in one batched run; `passes` from the
+plan read-back tells dense (0) from radix.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+import oracle
+from dbscan_torch import _C, dbscan2d, dbscan2d_batched, synthetic
+
+pytestmark = pytest.mark.gpu
+
+EPS = 0.5
+SIDE = EPS / np.sqrt(2.0)  # cell side
+
+
+def _rect(n, wx, wy, seed):
+    """n uniform points over about wx x wy cells."""
+    rng = np.random.default_rng(seed)
+    X = np.empty((n, 2), np.float32)
+    X[:, 0] = rng.uniform(0.0, wx * SIDE, n)
+    X[:, 1] = rng.uniform(0.0, wy * SIDE, n)
+    return X
+
+
+FORMS = [
+    # name, X, min_samples, dense
+    ("dense_W0.9M", _rect(300_000, 849, 849, 1), 3, True),
+    ("dense_W1.5M", _rect(500_000, 1500, 1000, 2), 3, True),
+    ("dense_W4.1M", _rect(1_200_000, 2000, 2000, 3), 3, True),
+    ("dense_W18M", _rect(5_000_000, 4500, 4000, 4), 3, True),
+    ("radix_sparse", _rect(100_000, 3000, 3000, 5), 2, False),     # W ~ 12M > 4N + 4096
+    ("hot_cell", synthetic.adversarial(400_000, seed=6), 4, True),  # half the points in a few cells
+]
+
+
+@pytest.mark.parametrize("name,X,ms,dense", FORMS, ids=[f[0] for f in FORMS])
+def test_sort_form_matches_oracle(name, X, ms, dense):
+    Xd = torch.from_numpy(X).cuda()
+    ours, info = _C.dbscan2d_info(Xd, EPS, ms)
+    assert (info["passes"] == 0) == dense, info
+    want = oracle.dbscan2d(X, EPS, ms)
+    got = ours.cpu().numpy()
+    diff = np.flatnonzero(got != want)
+    assert diff.size == 0, f"{name}: {diff.size}/{X.shape[0]} labels differ"
+    # A second run on the same workspace layout gives the same labels.
+    assert np.array_equal(dbscan2d(Xd, EPS, ms).cpu().numpy(), want)
+
+
+def test_batched_dense_clouds():
+    """Many dense clouds in one run: a thread's run of points crosses clouds,
+    so the per-cloud key parameters change inside the sort's point loops."""
+    rng = np.random.default_rng(7)
+    sizes = rng.integers(1, 20_000, size=60)
+    sizes[[3, 17]] = 0  # empty clouds in between
+    clouds = [synthetic.blobs_with_noise(int(s), seed=100 + k, n_blobs=3) if s else
+              np.zeros((0, 2), np.float32) for k, s in enumerate(sizes)]
+    eps = rng.uniform(0.3, 1.5, size=len(clouds))
+    ms = rng.integers(2, 12, size=len(clouds))
+    X = np.concatenate(clouds).astype(np.float32)
+    off = np.concatenate([[0], np.cumsum(sizes)])
+    lab = dbscan2d_batched(torch.from_numpy(X).cuda(), off.tolist(), eps.tolist(), ms.tolist()).cpu().numpy()
+    for k in range(len(clouds)):
+        want = oracle.dbscan2d(clouds[k], float(eps[k]), int(ms[k]))
+        assert np.array_equal(lab[off[k]:off[k + 1]], want), f"cloud {k}"
