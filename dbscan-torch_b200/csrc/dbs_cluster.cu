@@ -109,30 +109,35 @@ __device__ __forceinline__ int32_t uf_find_ro(const int32_t* uf, int32_t x, Desc
   return x;
 }
 
-// Path-halving find (relaxed writes only redirect to ancestors).
-__device__ __forceinline__ int32_t uf_find(int32_t* uf, int32_t x, Desc* d) {
-  volatile int32_t* vuf = uf;
-  int32_t px = vuf[x];
-  for (uint32_t it = 0; it < kFindCap; ++it) {
-    if (px == x) return x;
-    const int32_t gp = vuf[px];
-    vuf[x] = gp;
-    x = px;
-    px = gp;
-  }
-  set_error(d, kErrFind);
-  return x;
-}
-
-// Hook the larger root under the smaller (dbscan_cuda.cu:301-311), so the
-// root of every component is its smallest cell index.
+// Union of the sets of cells a and b. The reference (dbscan_cuda.cu:301-311)
+// finds both roots and hooks the larger under the smaller; here Rem's
+// algorithm with splicing does the same union: walk up from whichever side
+// has the larger parent, re-pointing it (compare-and-swap) at the other
+// side's smaller parent, until both sides share a parent (already one set) or
+// a root is reached and hooked. Every pointer only ever decreases
+// (uf[x] <= x), so the root of every component is its smallest cell index,
+// exactly as in the reference. Unlike root-to-root hooking, concurrent unions
+// of neighbouring sets cannot build long chains: a lattice of thousands of
+// sets merged at once (points at exactly eps) otherwise left finds walking
+// hundreds of links. A splice moves a subtree into the other endpoint's set;
+// the walk then continues from its old parent until that part is joined too,
+// so no union is lost.
 __device__ __forceinline__ void uf_unite(int32_t* uf, int32_t a, int32_t b, Desc* d) {
+  volatile int32_t* vuf = uf;
+  int32_t rx = a, ry = b;
   for (uint32_t it = 0; it < kFindCap; ++it) {
-    a = uf_find(uf, a, d);
-    b = uf_find(uf, b, d);
-    if (a == b) return;
-    const int32_t hi = a > b ? a : b, lo = a < b ? a : b;
-    if (atomicCAS(&uf[hi], hi, lo) == hi) return;
+    int32_t px = vuf[rx], py = vuf[ry];
+    if (px == py) return;
+    if (px < py) {
+      const int32_t t = rx; rx = ry; ry = t;
+      const int32_t u = px; px = py; py = u;
+    }
+    if (rx == px) {
+      if (atomicCAS(&uf[rx], rx, py) == rx) return;  // hook the root rx under py < rx
+    } else {
+      atomicCAS(&uf[rx], px, py);  // splice: py < px, then continue from px
+      rx = px;
+    }
   }
   set_error(d, kErrFind);
 }
