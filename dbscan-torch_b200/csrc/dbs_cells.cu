@@ -140,6 +140,13 @@ __device__ __forceinline__ int32_t find_cell(const Plan& p, const SegInfo& g, in
 
 constexpr int32_t kBigCell = 64;  // cells above this size reduce their box per warp
 
+// Box of a cell holding a point with a NaN coordinate (nan_box). fminf/fmaxf skip NaN,
+// so the folded box would leave that point out; the infinite box keeps every
+// prune sound (nothing is pruned against it) and turns off the whole-cell
+// shortcut of k_core, which would otherwise count the NaN point. No label
+// changes: a NaN point is within eps of nothing.
+__device__ __forceinline__ float4 nan_box() { return make_float4(-INFINITY, INFINITY, -INFINITY, INFINITY); }
+
 // Warp-aggregated append of the lanes with `take` to a work list.
 __device__ __forceinline__ void append_list(uint32_t* list, uint32_t* count, bool take, uint32_t v) {
   const uint32_t m = __ballot_sync(0xffffffffu, take);
@@ -182,16 +189,18 @@ __global__ void __launch_bounds__(kCellThreads) k_cell_prep(Plan p) {
       // through fminf/fmaxf.
       float2 v = p.xy[s0];
       float4 b = make_float4(v.x, v.x, v.y, v.y);
+      bool nan = isnan(v.x) || isnan(v.y);
       if (s1 - s0 > 1) {
         b = make_float4(fminf(v.x, INFINITY), fmaxf(v.x, -INFINITY), fminf(v.y, INFINITY),
                         fmaxf(v.y, -INFINITY));
         for (int32_t i = s0 + 1; i < s1; ++i) {
           v = p.xy[i];
+          nan |= isnan(v.x) || isnan(v.y);
           b.x = fminf(b.x, v.x); b.y = fmaxf(b.y, v.x);
           b.z = fminf(b.z, v.y); b.w = fmaxf(b.w, v.y);
         }
       }
-      p.bbox[c] = b;
+      p.bbox[c] = nan ? nan_box() : b;
     }
     if (huge) {
       // Registered for k_huge_bbox: one entry, ceil(size / kHugeChunk) chunks.
@@ -210,8 +219,10 @@ __global__ void __launch_bounds__(kCellThreads) k_cell_prep(Plan p) {
       bm &= bm - 1;
       const int32_t b0 = __shfl_sync(full, s0, l), b1 = __shfl_sync(full, s1, l);
       float xmin = INFINITY, xmax = -INFINITY, ymin = INFINITY, ymax = -INFINITY;
+      bool nan = false;
       for (int32_t i = b0 + lane; i < b1; i += 32) {
         const float2 v = p.xy[i];
+        nan |= isnan(v.x) || isnan(v.y);
         xmin = fminf(xmin, v.x); xmax = fmaxf(xmax, v.x);
         ymin = fminf(ymin, v.y); ymax = fmaxf(ymax, v.y);
       }
@@ -222,7 +233,8 @@ __global__ void __launch_bounds__(kCellThreads) k_cell_prep(Plan p) {
         ymin = fminf(ymin, __shfl_xor_sync(full, ymin, o));
         ymax = fmaxf(ymax, __shfl_xor_sync(full, ymax, o));
       }
-      if ((int)lane == l) p.bbox[c] = make_float4(xmin, xmax, ymin, ymax);
+      nan = __any_sync(full, nan);
+      if ((int)lane == l) p.bbox[c] = nan ? nan_box() : make_float4(xmin, xmax, ymin, ymax);
     }
 
     // Points of the warp's cells, runs of consecutive non-huge cells at a
@@ -323,6 +335,9 @@ __global__ void __launch_bounds__(256) k_huge_bbox(Plan p) {
         p.point_cell[i] = c;
         p.is_core[i] = dn ? 1 : 0;
         const float2 v = p.xy[i];
+        if (isnan(v.x) || isnan(v.y)) {  // whole box becomes nan_box()
+          xmin = -INFINITY; xmax = INFINITY; ymin = -INFINITY; ymax = INFINITY;
+        }
         xmin = fminf(xmin, v.x); xmax = fmaxf(xmax, v.x);
         ymin = fminf(ymin, v.y); ymax = fmaxf(ymax, v.y);
       }

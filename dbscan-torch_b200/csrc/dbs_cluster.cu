@@ -55,13 +55,20 @@ __global__ void __launch_bounds__(kCellThreads) k_core(Plan p) {
       int32_t cnt = st1 - st0;
       const float2 q = p.xy[i];
       const int32_t* row = p.ngh + (int64_t)c * kNgh;
+      // A neighbour cell wholly within eps of q (point_box_max_d2) counts all
+      // its points without distance tests: the same count.
       for (int off = 0; off < kNgh && cnt < ms; ++off) {
         if (off == 12) continue;
         const int32_t nb = row[off];
         if (nb < 0) continue;
-        if (!(point_box_d2(q.x, q.y, p.bbox[nb]) <= eps_sq)) continue;
-        const int32_t j1 = p.cell_start[nb + 1];
-        for (int32_t j = p.cell_start[nb]; j < j1; ++j) {
+        const float4 bb = p.bbox[nb];
+        if (!(point_box_d2(q.x, q.y, bb) <= eps_sq)) continue;
+        const int32_t j0 = p.cell_start[nb], j1 = p.cell_start[nb + 1];
+        if (point_box_max_d2(q.x, q.y, bb) <= eps_sq) {
+          cnt += j1 - j0;
+          continue;
+        }
+        for (int32_t j = j0; j < j1; ++j) {
           const float2 pj = p.xy[j];
           cnt += sq_dist(__fsub_rn(pj.x, q.x), __fsub_rn(pj.y, q.y)) <= eps_sq;
         }

@@ -202,6 +202,18 @@ __device__ __forceinline__ float point_box_d2(float x, float y, float4 b) {
   return sq_dist(dx, dy);
 }
 
+// Largest squared distance from (x, y) to a point of box b, in the same
+// rounded form as the pairwise test: every fsub and the fma are monotone in
+// the magnitudes of their operands, so for any point p inside b,
+// d2(p, (x, y)) <= point_box_max_d2(x, y, b). A cell whose box passes
+// `<= eps_sq` therefore has every point within eps (cells holding a NaN
+// coordinate carry an infinite box, which never passes).
+__device__ __forceinline__ float point_box_max_d2(float x, float y, float4 b) {
+  const float dx = fmaxf(fabsf(__fsub_rn(b.x, x)), fabsf(__fsub_rn(b.y, x)));
+  const float dy = fmaxf(fabsf(__fsub_rn(b.z, y)), fabsf(__fsub_rn(b.w, y)));
+  return sq_dist(dx, dy);
+}
+
 // dbscan_cuda.cu:190-194
 __device__ __forceinline__ float box_box_d2(float4 a, float4 b) {
   float dx = fmaxf(fmaxf(__fsub_rn(b.x, a.y), __fsub_rn(a.x, b.y)), 0.0f);

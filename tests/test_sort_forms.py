@@ -72,3 +72,30 @@ def test_batched_dense_clouds():
     for k in range(len(clouds)):
         want = oracle.dbscan2d(clouds[k], float(eps[k]), int(ms[k]))
         assert np.array_equal(lab[off[k]:off[k + 1]], want), f"cloud {k}"
+
+
+def _with_specials(kind, seed):
+    X = synthetic.blobs_with_noise(60_000, seed=seed, n_blobs=6)
+    rng = np.random.default_rng(seed)
+    idx = rng.choice(X.shape[0], size=40, replace=False)
+    if kind == "nan":
+        X[idx[:20], 0] = np.nan
+        X[idx[20:], 1] = np.nan
+    else:
+        X[idx[:20], 0] = np.inf
+        X[idx[20:], 1] = -np.inf
+    return X
+
+
+@pytest.mark.parametrize("kind", ["nan", "inf"])
+def test_special_coordinates(kind):
+    """Points with a NaN or infinite coordinate: cells holding them get an
+    infinite box (NaN) or a huge key range (inf, radix sort); the labels stay
+    those of the oracle and, when present, of the reference CUDA build."""
+    import refmod
+    X = _with_specials(kind, 11)
+    ours = dbscan2d(torch.from_numpy(X).cuda(), EPS, 5).cpu().numpy()
+    assert np.array_equal(ours, oracle.dbscan2d(X, EPS, 5))
+    ref = refmod.load("cuda")
+    if ref is not None:
+        assert np.array_equal(ours, ref.dbscan2d(torch.from_numpy(X).cuda(), EPS, 5).cpu().numpy())
