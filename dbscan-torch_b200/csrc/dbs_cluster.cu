@@ -215,9 +215,9 @@ __constant__ int8_t kRingOffs[2][16] = {
 // flatten so that most of its pairs are already connected):
 //   k_pairs       one thread per core cell: its neighbours nc > c of the
 //                 ring that are core cells and pass the box-box prune
-//                 (dbscan_cuda.cu:329-351); with `skip_united` pairs already
-//                 in one component (read-only finds) are dropped. Survivors
-//                 go to a pair list.
+//                 (dbscan_cuda.cu:329-351); with `skip_united` (after a
+//                 flatten) pairs already in one component are dropped.
+//                 Survivors go to a pair list.
 //   k_pair_scan   one thread per listed pair: i over c's core points passing
 //                 the point-box prune against nc, j over nc's core points,
 //                 early exit on the first pair within eps (:353-368); found
@@ -247,8 +247,10 @@ __global__ void __launch_bounds__(256) k_pairs(Plan p, int ring, int skip_united
         if (nb <= (int32_t)c || p.cell_status[nb] == 0) continue;
         if (!(box_box_d2(bb_c, p.bbox[nb]) <= eps_sq)) continue;
         if (skip_united) {
-          if (root_c < 0) root_c = uf_find_ro(p.uf, (int32_t)c, d);
-          if (uf_find_ro(p.uf, nb, d) == root_c) continue;
+          // The flatten just before left every cell pointing at its root,
+          // and no union runs during this kernel: one load is the find.
+          if (root_c < 0) root_c = p.uf[c];
+          if (p.uf[nb] == root_c) continue;
         }
         mask |= 1u << k;
       }

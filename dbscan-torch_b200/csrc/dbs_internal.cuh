@@ -7,17 +7,19 @@
 //
 //   k_init         zero per-call counters, histograms, per-cloud bounds
 //   k_bounds       per-cloud bounds of the cell coordinates (kx, ky)
-//   k_seg_finalize per-cloud compacted key ranges, key bases, pass count
-//   k_keys         compacted cell keys + first-digit histogram per chunk
-//   k_sort_* x8    LSD radix passes (count, scan, scatter); passes past the
-//                  device-side pass count return at once; the last real pass
-//                  also gathers the sorted float2 coordinates and perm
-//   k_rle          run-length cells: cell_start, cell_key, cell map
-//   k_cell_prep    per-cell bounding box + 25-entry neighbour table
-//   k_core         core flags (warp-cooperative counts) + cell status
-//   k_union        cell-graph union-find over core cells
+//   k_seg_finalize per-cloud compacted key ranges, key bases, sort form
+//   k_csort        dense key spaces: counting sort, cells, dense cell map
+//   k_keys, k_radix  otherwise: keys + LSD radix sort (return at once when
+//                  the counting sort ran, and k_csort returns when they run)
+//   k_rle          run-length cells after the radix sort
+//   k_cell_prep    per-cell box + 25-entry neighbour row; point classes
+//   k_core         core flags of the query points
+//   k_status       cell status, union-find init
+//   k_pairs / k_pair_scan / k_pair_warp (two rings, k_flatten between)
+//                  cell-graph union-find over core cells
 //   k_ids          flatten + exclusive scan of root flags (look-back)
-//   k_labels       core labels, border assignment, unpermute
+//   k_cid          cluster id per cell
+//   k_labels       border assignment, core labels, unpermute
 //
 // The plain call is the batched call with one cloud: every kernel works on
 // a segmented layout (clouds concatenated, each with its own eps and

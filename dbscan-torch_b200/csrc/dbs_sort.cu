@@ -1,4 +1,4 @@
-// dbs_sort.cu -- grid hashing and the LSD onesweep radix sort.
+// dbs_sort.cu -- per-cloud key layout and the LSD radix sort.
 //
 // Reference path replaced (ryanirl/dbscan-torch v0.2.0, csrc/cuda/dbscan_cuda.cu):
 //   k_cell_keys :55-66, thrust::sort_by_key :582-586, k_gather_xy :71-79.
@@ -14,13 +14,13 @@
 // 10M-point constant-density cloud instead of eight passes. Keys are stored
 // as u32 when they fit, else u64 (decided on the device).
 //
-// Sort. One histogram pass computes every digit's 256-bin histogram; each
-// onesweep pass then ranks a 4096-key tile in shared memory (warp match
-// ranking, stable), resolves its global digit offsets by decoupled look-back
-// over per-(tile, digit) words, and scatters through a shared-memory staging
-// buffer so each digit run is written contiguously. Tiles are taken in
-// launch order from an atomic counter, so a tile only waits on tiles whose
-// blocks are already running. The last pass writes perm and gathers the
+// Sort (clouds whose key range is sparse, and the debug entry point; dense
+// key spaces take the counting sort of dbs_csort.cu): k_keys writes the keys
+// and the first digit's counts per chunk; k_radix, one cooperative kernel,
+// runs the LSD passes with 8-bit digits -- per-digit scan of the chunk counts,
+// then each chunk ranks each 4096-key tile in shared memory (ballot-based,
+// stable) and scatters through a shared-memory staging buffer so each digit
+// run is written contiguously. The last pass writes perm and gathers the
 // float2 coordinates (the reference's k_gather_xy) in the same scatter.
 #include "dbs_internal.cuh"
 
