@@ -17,6 +17,13 @@ synthetic data. One step = one dbscan2d call over the whole cloud.
   cpu_baseline  the reference's own CPU implementation (built from its
             sources into oracle/_ref/cpu) on the box's host cores, timed on
             the same workload
+  batched   4,096 clouds (sizes log-uniform in [256, 262144]) in one batched
+            pipeline run vs a loop of plain calls: clouds/s of each
+            (--batched-clouds; 0 skips)
+  serving   a Poisson request stream (2,000 req/s, sizes log-uniform in
+            [1e3, 2e6]) through the continuous-batching server vs sequential
+            plain calls: p50/p99 latency and clouds/s (--serve-seconds,
+            default 10 s of arrivals; 0 skips)
 
 --impl reference times only that reference CPU path and prints its line.
 Multi-GPU (torchrun): replicas only -- every rank clusters its own cloud;
@@ -327,8 +334,132 @@ def run_ours(args, world, rank, local):
            "roofline": roof}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(X_np, EPS, MIN_SAMPLES)
-    del labels
+    del labels, X, flush, X_host
+    torch.cuda.empty_cache()
+    if world == 1:
+        if args.batched_clouds > 0:
+            out["batched"] = run_batched(dev, args.batched_clouds)
+        if args.serve_seconds > 0:
+            out["serving"] = run_serving(dev, args.serve_seconds)
     return out
+
+
+def _ev_ms(fn):
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record()
+    out = fn()
+    b.record()
+    torch.cuda.synchronize()
+    return a.elapsed_time(b), out
+
+
+def run_batched(dev, n_clouds: int) -> dict:
+    """Config 3: n_clouds independent clouds (sizes log-uniform in [256, 262144],
+    eps_i in [0.2, 1.0], min_samples_i in {4..32}) clustered by one batched
+    pipeline run, against a loop of plain calls over the same device-resident
+    clouds. Both timed with CUDA events; labels compared cloud by cloud."""
+    from dbscan_torch import dbscan2d, dbscan2d_batched, synthetic
+    rng = np.random.default_rng(0)
+    sizes = np.exp(rng.uniform(np.log(256), np.log(262_144), size=n_clouds)).astype(np.int64)
+    eps = rng.uniform(0.2, 1.0, size=n_clouds)
+    ms = rng.integers(4, 33, size=n_clouds)
+    X, off = synthetic.blobs_with_noise_device(sizes, seed=0, device=dev)
+    offl = off.tolist()
+    dbscan2d_batched(X, off, eps, ms)  # warm-up
+    tb = []
+    for _ in range(3):
+        t, lab_b = _ev_ms(lambda: dbscan2d_batched(X, off, eps, ms))
+        tb.append(t)
+
+    def loop():
+        return [dbscan2d(X[offl[k]:offl[k + 1]], float(eps[k]), int(ms[k])) for k in range(n_clouds)]
+
+    loop()  # warm-up: the caching allocator holds every workspace size afterwards
+    tp, labs = _ev_ms(loop)
+    equal = all(torch.equal(labs[k], lab_b[offl[k]:offl[k + 1]]) for k in range(n_clouds))
+    _C_check()
+    t_b = statistics.median(tb)
+    n_pts = int(offl[-1])
+    del X, lab_b, labs
+    torch.cuda.empty_cache()
+    return {"workload": f"{n_clouds} clouds, N_i log-uniform [256, 262144], eps_i U[0.2, 1.0], "
+                        f"min_samples_i U{{4..32}} (device generator, seed 0)",
+            "clouds": n_clouds, "points": n_pts,
+            "batched_ms": round(t_b, 3), "batched_clouds_per_s": round(n_clouds / (t_b * 1e-3), 1),
+            "batched_mpoints_per_s": round(n_pts / (t_b * 1e-3) / 1e6, 1),
+            "plain_loop_ms": round(tp, 3), "plain_loop_clouds_per_s": round(n_clouds / (tp * 1e-3), 1),
+            "speedup": round(tp / t_b, 2), "labels_equal": bool(equal)}
+
+
+def _C_check():
+    from dbscan_torch import check_status
+    check_status()
+
+
+def run_serving(dev, seconds: float, rate_hz: float = 2000.0, budget_bytes: int = 64 << 30) -> dict:
+    """Config 4: Poisson arrivals at rate_hz for `seconds`, sizes log-uniform in
+    [1e3, 2e6] (prefixes of shuffled 2M-point clouds of the config-0
+    distribution, pinned on the host), eps U[0.1, 1.0], min_samples U{4..32}.
+    The continuous-batching server (64 GiB admission budget) against
+    sequential plain calls on the same stream; latency = completion minus
+    arrival, host clock."""
+    from dbscan_torch import DbscanServer, dbscan2d, synthetic
+    arrivals, sizes, eps, ms, _ = synthetic.request_stream(rate_hz=rate_hz, duration_s=seconds, seed=0)
+    pool_n, pool_k = 2_000_000, 8
+    pool_d, pool_off = synthetic.blobs_with_noise_device([pool_n] * pool_k, seed=1, device=dev)
+    pool = pool_d.cpu().pin_memory()
+    del pool_d
+    reqs_x = [pool[int(pool_off[k % pool_k]): int(pool_off[k % pool_k]) + int(sizes[k])]
+              for k in range(len(sizes))]
+    n = len(reqs_x)
+
+    srv = DbscanServer(budget_bytes=budget_bytes, lane_points=16 << 20, lane_clouds=256)
+    for k in range(8):  # warm-up batch
+        srv.submit(reqs_x[k], float(eps[k]), int(ms[k]))
+    srv.drain()
+    srv.batches = srv.completed = 0
+    reqs = []
+    t0 = time.perf_counter()
+    i = 0
+    while i < n or srv.queue or any(l.busy for l in srv.lanes):
+        now = time.perf_counter() - t0
+        while i < n and arrivals[i] <= now:
+            reqs.append(srv.submit(reqs_x[i], float(eps[i]), int(ms[i]), t_submit=t0 + arrivals[i]))
+            i += 1
+        if srv.step() == 0:
+            time.sleep(20e-6)
+    t_end = max(r.t_done for r in reqs) - t0
+    lat_s = np.array([r.latency for r in reqs]) * 1e3
+
+    for k in range(8):  # warm-up of the plain path
+        dbscan2d(reqs_x[k], float(eps[k]), int(ms[k]))
+    lat_p = np.empty(n)
+    sample = {}
+    t0 = time.perf_counter()
+    for k in range(n):
+        while time.perf_counter() - t0 < arrivals[k]:
+            pass
+        lab = dbscan2d(reqs_x[k], float(eps[k]), int(ms[k]))
+        lat_p[k] = (time.perf_counter() - t0 - arrivals[k]) * 1e3
+        if k % 97 == 0:
+            sample[k] = lab
+    t_end_p = time.perf_counter() - t0
+    equal = all(torch.equal(reqs[k].labels, lab) for k, lab in sample.items())
+    batches = srv.batches
+    del pool, reqs_x, reqs, srv
+    torch.cuda.empty_cache()
+    pct = lambda a, q: round(float(np.percentile(a, q)), 3)
+    return {"workload": f"Poisson {rate_hz:g} req/s for {seconds:g} s, N log-uniform [1e3, 2e6], "
+                        f"eps U[0.1, 1.0], min_samples U{{4..32}}",
+            "requests": n, "mean_points": round(float(np.mean(sizes)), 1),
+            "budget_gb": round(budget_bytes / 2**30, 1), "arena_gb": round(
+                (2 * __import__("dbscan_torch").footprint_bytes(16 << 20, 256)) / 2**30, 2),
+            "server": {"p50_ms": pct(lat_s, 50), "p99_ms": pct(lat_s, 99),
+                       "clouds_per_s": round(n / t_end, 1), "batches": batches},
+            "sequential_plain": {"p50_ms": pct(lat_p, 50), "p99_ms": pct(lat_p, 99),
+                                 "clouds_per_s": round(n / t_end_p, 1)},
+            "labels_equal_sampled": bool(equal)}
 
 
 def main():
@@ -338,6 +469,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batched-clouds", type=int, default=4096,
+                    help="clouds of the batched comparison (0 skips it)")
+    ap.add_argument("--serve-seconds", type=float, default=10.0,
+                    help="length of the serving stream (0 skips it)")
     args = ap.parse_args()
     world, rank, local = dist_setup(args.gpus)
     try:

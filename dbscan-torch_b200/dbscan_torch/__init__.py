@@ -57,7 +57,7 @@ ArrayLike2D = Union[np.ndarray, torch.Tensor]
 
 __all__ = [
     "dbscan2d", "dbscan2d_profile", "dbscan2d_batched", "DBSCAN", "ArrayLike2D",
-    "BatchedPlan", "check_status",
+    "BatchedPlan", "DbscanServer", "footprint_bytes", "check_status",
 ]
 
 try:
@@ -145,3 +145,4 @@ class DBSCAN:
 
 
 from .batched import BatchedPlan  # noqa: E402  (needs _C)
+from .serve import DbscanServer, footprint_bytes  # noqa: E402  (needs _C)

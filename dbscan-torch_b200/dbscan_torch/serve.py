@@ -1,0 +1,235 @@
+"""Serving loop: many independent clustering requests under a device-memory
+budget, continuously batched into segmented pipeline runs.
+
+No counterpart in the reference (it clusters one cloud per call). Each
+request has the semantics of a plain ``dbscan2d`` call on its own cloud: its
+labels are numbered from 0 and equal that call's labels bit for bit.
+
+Structure:
+
+* **Arena.** ``lanes`` (default 2) fixed sets of device buffers, allocated
+  once: points, labels, per-cloud tables and one pipeline workspace, each set
+  sized for ``lane_points`` points and ``lane_clouds`` clouds. The whole arena
+  (``arena_bytes``) stays under ``budget_bytes``. Each lane has its own
+  stream, so one batch runs while the next is assembled.
+* **Footprint and admission.** ``footprint_bytes(n)`` is what a request of n
+  points occupies in a lane (workspace share plus points and labels). A
+  request joins a batch while the batch's points and cloud count fit the lane;
+  a request larger than a whole lane is refused at ``submit``.
+* **Continuous batching.** ``step()`` retires finished batches and, whenever a
+  lane is free and requests are queued, launches every queued request that
+  fits (first come, first served) as one batched pipeline run: one
+  host-to-device copy per request into the lane's point buffer, one copy of
+  the cloud tables, the segmented pipeline, one device-to-host copy of all
+  labels and of the device status word. Completion is observed through CUDA
+  events, never by blocking the host.
+
+Host inputs should be pinned (``torch.Tensor.pin_memory()``) for the copies
+to be asynchronous.
+"""
+
+from __future__ import annotations
+
+import collections
+import time
+from dataclasses import dataclass, field
+from typing import Deque, List, Optional
+
+import numpy as np
+import torch
+
+from . import _C
+
+
+def footprint_bytes(n: int, nseg: int = 1) -> int:
+    """Device bytes a batch of ``nseg`` clouds holding ``n`` points occupies:
+    pipeline workspace, float32 (n, 2) points and int32 labels."""
+    return int(_C.workspace_bytes(max(int(n), 1), max(int(nseg), 1))) + 12 * int(n) + 24 * int(nseg)
+
+
+@dataclass
+class Request:
+    """One clustering request. ``labels`` (a CPU int32 tensor) is set when
+    ``done``; ``t_submit`` / ``t_done`` are ``time.perf_counter()`` stamps."""
+    X: torch.Tensor
+    eps: float
+    min_samples: int
+    t_submit: float
+    rid: int
+    labels: Optional[torch.Tensor] = None
+    t_done: float = 0.0
+    done: bool = False
+
+    @property
+    def n(self) -> int:
+        return int(self.X.shape[0])
+
+    @property
+    def latency(self) -> float:
+        return self.t_done - self.t_submit
+
+
+@dataclass
+class _Lane:
+    stream: torch.cuda.Stream
+    X: torch.Tensor
+    labels: torch.Tensor
+    offsets: torch.Tensor
+    params: torch.Tensor
+    ws: torch.Tensor
+    labels_host: torch.Tensor
+    offsets_host: torch.Tensor
+    params_host: torch.Tensor
+    status_host: torch.Tensor
+    event: torch.cuda.Event
+    batch: List[Request] = field(default_factory=list)
+    busy: bool = False
+
+
+class DbscanServer:
+    """Continuous-batching DBSCAN server on one device (see module docstring).
+
+    Args:
+        budget_bytes: device memory the arena may use (default 64 GiB).
+        lane_points: points per lane; default: the largest that keeps the
+            arena under the budget, capped at 64M points.
+        lane_clouds: clouds per lane (per batch).
+        lanes: number of lanes (concurrent batches).
+    """
+
+    def __init__(self, budget_bytes: int = 64 << 30, lane_points: Optional[int] = None,
+                 lane_clouds: int = 1024, lanes: int = 2, device=None):
+        self.device = torch.device(device) if device is not None else torch.device(
+            "cuda", torch.cuda.current_device())
+        if lanes < 1 or lane_clouds < 1:
+            raise ValueError("lanes and lane_clouds must be >= 1")
+        per_lane = budget_bytes // lanes
+        if lane_points is None:
+            lo, hi = 1, 64 << 20
+            while lo < hi:  # largest lane_points whose footprint fits per_lane
+                mid = (lo + hi + 1) // 2
+                if footprint_bytes(mid, lane_clouds) <= per_lane:
+                    lo = mid
+                else:
+                    hi = mid - 1
+            lane_points = lo
+        if footprint_bytes(lane_points, lane_clouds) > per_lane:
+            raise ValueError(f"a lane of {lane_points} points and {lane_clouds} clouds needs "
+                             f"{footprint_bytes(lane_points, lane_clouds)} bytes, more than "
+                             f"budget_bytes / lanes = {per_lane}")
+        self.budget_bytes = int(budget_bytes)
+        self.lane_points = int(lane_points)
+        self.lane_clouds = int(lane_clouds)
+        self.arena_bytes = lanes * footprint_bytes(lane_points, lane_clouds)
+        self.lanes: List[_Lane] = []
+        for _ in range(lanes):
+            P, S, d = self.lane_points, self.lane_clouds, self.device
+            self.lanes.append(_Lane(
+                stream=torch.cuda.Stream(device=d),
+                X=torch.zeros((P, 2), dtype=torch.float32, device=d),
+                labels=torch.empty(P, dtype=torch.int32, device=d),
+                offsets=torch.zeros(S + 1, dtype=torch.int64, device=d),
+                params=torch.zeros(S * 16, dtype=torch.uint8, device=d),
+                ws=torch.empty(int(_C.workspace_bytes(P, S)), dtype=torch.uint8, device=d),
+                labels_host=torch.empty(P, dtype=torch.int32).pin_memory(),
+                offsets_host=torch.zeros(S + 1, dtype=torch.int64).pin_memory(),
+                params_host=torch.zeros(S * 16, dtype=torch.uint8).pin_memory(),
+                status_host=torch.zeros(4, dtype=torch.uint8).pin_memory(),
+                event=torch.cuda.Event(),
+            ))
+        self.queue: Deque[Request] = collections.deque()
+        self._next_id = 0
+        self.batches = 0
+        self.completed = 0
+
+    # ------------------------------------------------------------- requests
+    def submit(self, X: torch.Tensor, eps: float, min_samples: int, t_submit: Optional[float] = None) -> Request:
+        """Queue one cloud (float32 (N, 2) CPU tensor, ideally pinned)."""
+        if X.dim() != 2 or X.size(1) != 2:
+            raise RuntimeError("X must have shape (N, 2)")
+        if X.dtype != torch.float32:
+            raise RuntimeError("X must be float32")
+        if not eps > 0:
+            raise RuntimeError("eps must be > 0")
+        if min_samples < 1:
+            raise RuntimeError("min_samples must be >= 1")
+        if X.size(0) > self.lane_points:
+            raise RuntimeError(f"request of {X.size(0)} points exceeds the lane capacity of "
+                               f"{self.lane_points} points (budget {self.budget_bytes} bytes)")
+        r = Request(X=X.contiguous(), eps=float(eps), min_samples=int(min_samples),
+                    t_submit=time.perf_counter() if t_submit is None else t_submit, rid=self._next_id)
+        self._next_id += 1
+        self.queue.append(r)
+        return r
+
+    # ----------------------------------------------------------------- loop
+    def step(self) -> int:
+        """Retire finished batches, launch new ones on free lanes. Returns the
+        number of requests completed by this call. Never blocks on the GPU."""
+        done = 0
+        for lane in self.lanes:
+            if lane.busy and lane.event.query():
+                done += self._retire(lane)
+        for lane in self.lanes:
+            if not lane.busy and self.queue:
+                self._launch(lane)
+        return done
+
+    def drain(self) -> None:
+        """Run until every submitted request is done."""
+        while self.queue or any(l.busy for l in self.lanes):
+            if self.step() == 0:
+                time.sleep(20e-6)
+
+    def _launch(self, lane: _Lane) -> None:
+        batch: List[Request] = []
+        total = 0
+        while self.queue and len(batch) < self.lane_clouds and total + self.queue[0].n <= self.lane_points:
+            r = self.queue.popleft()
+            batch.append(r)
+            total += r.n
+        if not batch:
+            return
+        S = len(batch)
+        sizes = np.fromiter((r.n for r in batch), dtype=np.int64, count=S)
+        off = np.zeros(S + 1, dtype=np.int64)
+        np.cumsum(sizes, out=off[1:])
+        lane.offsets_host[: S + 1].copy_(torch.from_numpy(off))
+        eps = torch.tensor([r.eps for r in batch], dtype=torch.float64)
+        ms = torch.tensor([r.min_samples for r in batch], dtype=torch.int64)
+        lane.params_host[: S * 16].copy_(_C.fill_seg_params(eps, ms))
+        with torch.cuda.stream(lane.stream):
+            # The previous batch's host copies of this lane are complete (the
+            # lane was retired), so its pinned buffers can be rewritten.
+            lane.offsets[: S + 1].copy_(lane.offsets_host[: S + 1], non_blocking=True)
+            lane.params[: S * 16].copy_(lane.params_host[: S * 16], non_blocking=True)
+            for k, r in enumerate(batch):
+                if r.n:
+                    lane.X[off[k]: off[k + 1]].copy_(r.X, non_blocking=True)
+            if total:
+                _C.dbscan2d_batched_into(lane.X[:total], lane.offsets[: S + 1], lane.params[: S * 16],
+                                         lane.labels[:total], lane.ws)
+                lane.labels_host[:total].copy_(lane.labels[:total], non_blocking=True)
+                lane.status_host.copy_(lane.ws[:4], non_blocking=True)
+            lane.event.record(lane.stream)
+        lane.batch = batch
+        lane.busy = True
+        self.batches += 1
+
+    def _retire(self, lane: _Lane) -> int:
+        st = int(lane.status_host.view(torch.int32)[0]) if lane.batch and sum(r.n for r in lane.batch) else 0
+        if st:
+            raise RuntimeError(f"dbscan2d (serving): device-side failure (status 0x{st:x}) in a batch of "
+                               f"{len(lane.batch)} requests; their labels are invalid")
+        now = time.perf_counter()
+        pos = 0
+        for r in lane.batch:
+            r.labels = lane.labels_host[pos: pos + r.n].clone()
+            pos += r.n
+            r.t_done = now
+            r.done = True
+        n = len(lane.batch)
+        self.completed += n
+        lane.batch = []
+        lane.busy = False
+        return n

@@ -24,6 +24,7 @@ All outputs are float32 (N, 2) numpy arrays, shuffled.
 from __future__ import annotations
 
 import numpy as np
+import torch
 
 
 def blobs_with_noise(n: int = 100_000, seed: int = 0, n_blobs: int = 20,
@@ -113,3 +114,46 @@ def request_stream(rate_hz: float = 2000.0, duration_s: float = 60.0, seed: int 
     ms = rng.integers(ms_range[0], ms_range[1] + 1, size=n_req)
     seeds = rng.integers(0, 2**31 - 1, size=n_req)
     return arrivals, sizes, eps, ms, seeds
+
+
+def blobs_with_noise_device(sizes, seed: int = 0, device="cuda", n_blobs: int = 20,
+                            noise_frac: float = 0.05):
+    """Many clouds with the distribution of ``blobs_with_noise``, generated on
+    the device in one pass (the numpy generator's row shuffle takes minutes
+    for ~10^8 points). Cloud k has ``sizes[k]`` points: ``n_blobs`` Gaussian
+    blobs (sigma 1) with centres uniform in [-50, 50]^2 and equal mass (the
+    first ``n_blob % n_blobs`` blobs one point larger), plus
+    ``round(noise_frac * n)`` uniform points over [-60, 60]^2, shuffled within
+    the cloud. Seeded (torch's device generator), so repeatable on one GPU
+    type; the random streams differ from the numpy generator's.
+
+    Returns (X float32 (sum(sizes), 2) on ``device``, offsets int64 (S + 1,)
+    on the host)."""
+    dev = torch.device(device)
+    sizes = torch.as_tensor(np.asarray(sizes, dtype=np.int64))
+    S = sizes.numel()
+    off = torch.zeros(S + 1, dtype=torch.int64)
+    off[1:] = torch.cumsum(sizes, 0)
+    N = int(off[-1])
+    g = torch.Generator(device=dev)
+    g.manual_seed(int(seed))
+    sizes_d = sizes.to(dev)
+    cloud = torch.repeat_interleave(torch.arange(S, device=dev), sizes_d)
+    j = torch.arange(N, device=dev) - off.to(dev)[cloud]
+    n_noise = torch.round(sizes_d.double() * noise_frac).long()
+    n_blob = sizes_d - n_noise
+    per = n_blob // n_blobs
+    rem = n_blob - per * n_blobs
+    boundary = rem * (per + 1)
+    jb = j
+    blob = torch.where(jb < boundary[cloud], jb // (per[cloud] + 1),
+                       rem[cloud] + (jb - boundary[cloud]) // per[cloud].clamp(min=1))
+    blob = blob.clamp(max=n_blobs - 1)
+    centers = torch.rand((S, n_blobs, 2), generator=g, device=dev, dtype=torch.float64) * 100.0 - 50.0
+    pts = centers[cloud, blob] + torch.randn((N, 2), generator=g, device=dev, dtype=torch.float64)
+    noise = torch.rand((N, 2), generator=g, device=dev, dtype=torch.float64) * 120.0 - 60.0
+    X = torch.where((j < n_blob[cloud])[:, None], pts, noise).to(torch.float32)
+    del pts, noise, blob, jb
+    key = cloud.double() + torch.rand(N, generator=g, device=dev, dtype=torch.float64)
+    order = torch.argsort(key)
+    return X[order].contiguous(), off
