@@ -306,8 +306,12 @@ def run_ours(args, world, rank, local):
 
     # End to end through the public API with host buffers.
     X_host = torch.from_numpy(X_np).pin_memory()
-    for _ in range(2):
-        dbscan2d(X_host, EPS, MIN_SAMPLES)
+    # Warm-up keeps each result alive until the next call returns, as the
+    # timed loop does, so the caching host allocator holds both pinned label
+    # blocks before timing starts.
+    lab_host = None
+    for _ in range(3):
+        lab_host = dbscan2d(X_host, EPS, MIN_SAMPLES)
     e2e_ms = []
     for k in range(args.steps):
         flush.fill_(float(k))

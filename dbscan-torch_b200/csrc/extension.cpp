@@ -43,10 +43,14 @@ void check_rc(int rc, const char* what) {
 }
 
 // ---------------------------------------------------------- status checks
+// The workspace itself is not held until its status word is read: the copy
+// of the status word is enqueued on the stream the workspace was allocated on,
+// and the caching allocator hands a freed block only to later work on that
+// same stream, which runs after the copy. (Holding it made every call of a
+// host running ahead of the device allocate a fresh workspace.)
 struct PendingStatus {
   cudaEvent_t ev = nullptr;
   uint32_t* host = nullptr;  // pinned
-  torch::Tensor ws;          // keeps the workspace alive until read
   bool busy = false;
 };
 
@@ -70,7 +74,6 @@ void drain(bool wait) {
     if (q == cudaErrorNotReady) continue;
     C10_CUDA_CHECK(q);
     s.busy = false;
-    s.ws = torch::Tensor();
     const uint32_t st = *s.host;
     raise_if_failed(st);
   }
@@ -89,7 +92,6 @@ void enqueue_status(const torch::Tensor& ws, cudaStream_t stream) {
     PendingStatus& s = g_slots[g_next];
     C10_CUDA_CHECK(cudaEventSynchronize(s.ev));
     s.busy = false;
-    s.ws = torch::Tensor();
     raise_if_failed(*s.host);
     slot = &s;
     g_next = (g_next + 1) % kSlots;
@@ -104,7 +106,6 @@ void enqueue_status(const torch::Tensor& ws, cudaStream_t stream) {
   C10_CUDA_CHECK(cudaMemcpyAsync(slot->host, ws.data_ptr(), sizeof(uint32_t),
                                  cudaMemcpyDeviceToHost, stream));
   C10_CUDA_CHECK(cudaEventRecord(slot->ev, stream));
-  slot->ws = ws;
   slot->busy = true;
 }
 
