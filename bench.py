@@ -55,14 +55,14 @@ WORKLOAD = "constant_density_10M"
 L2_FLUSH_BYTES = 512 << 20
 # Kernel launches of one dbscan2d call (tests/test_launch_count.py counts them
 # with the profiler): init, bounds, seg_finalize | csort, keys, radix | rle |
-# cell_prep, huge_bbox | core, status | 2 x (pairs_reset, pairs, pair_scan,
-# pair_warp) + flatten | ids, cid | labels. Kernels whose work the
+# cell_prep, huge_bbox | core, status | 2 x (pairs, pair_scan, pair_warp) +
+# flatten | ids, cid | labels. Kernels whose work the
 # device-side plan skips (radix passes under the counting sort, the huge-cell
 # pass without huge cells) still launch and return at once.
-KERNELS_PER_CALL = 23
+KERNELS_PER_CALL = 21
 # Launches per reference stage (the profile entry point times stages).
 STAGE_LAUNCHES = {"cell_keys": 3, "sort_gather": 3, "boundary_scan": 1, "build_ngh": 2,
-                  "core_mark": 2, "union_find": 9, "cluster_id": 2, "border_assign": 1}
+                  "core_mark": 2, "union_find": 7, "cluster_id": 2, "border_assign": 1}
 # The kernel that does a stage's work when one kernel does (the others of the
 # stage return at once on this workload).
 STAGE_KERNEL = {"sort_gather": "k_csort", "build_ngh": "k_cell_prep", "border_assign": "k_labels"}

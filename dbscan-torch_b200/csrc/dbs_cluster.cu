@@ -7,11 +7,13 @@
 //   thrust::exclusive_scan :698-701, k_cluster_id_per_cell :392-404,
 //   k_core_labels :409-417, k_border_assign :427-470, k_unpermute :475-481.
 //
-// Core marking and labelling run one thread per sorted point, so the threads
-// of a warp are consecutive points, mostly of one cell: the neighbour row,
-// boxes and candidate points they read are the same addresses. Union-find
-// gives one warp to one core cell and one lane to each stencil neighbour.
-// The reference's bounding-box prunes are kept exactly, so every pair the
+// Core marking runs one thread per query point (the points of cells below
+// min_samples, listed by k_cell_prep in sorted order, so a warp's threads are
+// mostly points of one cell and share its neighbour row, boxes and candidate
+// points). Union-find works on compacted cell-pair lists: one thread per
+// candidate pair, one warp per pair over the thread's test budget. Labelling
+// runs one thread per border point, then one per sorted point. The
+// reference's bounding-box prunes are kept exactly, so every pair the
 // reference tests is tested with the same arithmetic and the same verdict.
 #include "dbs_internal.cuh"
 
@@ -328,9 +330,14 @@ __global__ void __launch_bounds__(256) k_pair_warp(Plan p) {
 // Point every cell at its current root (read-only walks: a concurrent
 // writer of uf[c] only ever stores an ancestor of c, so walks still end at
 // the root).
+// Between the rings: every cell to its root (so a find in ring 2's pair
+// listing is one load), and the pair lists emptied for ring 2 (ring 1 starts
+// from the counters k_init cleared; ring 1's k_pair_warp, which reads them,
+// has finished when this kernel runs).
 __global__ void __launch_bounds__(256) k_flatten(Plan p) {
   Desc* d = p.desc;
   const uint32_t C = d->num_cells;
+  if (blockIdx.x == 0 && threadIdx.x == 0) { d->p_count = 0; d->d_count = 0; }
   for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < C; c += gridDim.x * blockDim.x)
     p.uf[c] = uf_find_ro(p.uf, (int32_t)c, d);
 }
@@ -354,14 +361,35 @@ __global__ void __launch_bounds__(kScanThreads) k_ids(Plan p) {
     const int64_t tile = s_tile;
     if (tile >= tiles) break;
     const int64_t c0 = tile * kScanTile + (int64_t)threadIdx.x * kScanItems;
+    // Roots of the thread's cells, the walks advanced in lockstep: each round
+    // issues one independent load per unfinished walk instead of finishing
+    // one walk before starting the next.
+    int32_t r[kScanItems];
+    uint32_t open = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+      const int64_t c = c0 + k;
+      r[k] = c < C ? p.uf[c] : (int32_t)c;
+      if (c < C && r[k] != (int32_t)c) open |= 1u << k;
+    }
+    for (uint32_t it = 0; open && it < kFindCap; ++it) {
+      int32_t nx[kScanItems];
+#pragma unroll
+      for (int k = 0; k < kScanItems; ++k) nx[k] = (open >> k) & 1u ? p.uf[r[k]] : r[k];
+#pragma unroll
+      for (int k = 0; k < kScanItems; ++k) {
+        if (nx[k] == r[k]) open &= ~(1u << k);
+        r[k] = nx[k];
+      }
+    }
+    if (open) set_error(d, kErrFind);
     uint32_t flags = 0, cnt = 0;
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k) {
       const int64_t c = c0 + k;
       if (c < C) {
-        const int32_t r = uf_find_ro(p.uf, (int32_t)c, d);
-        p.uf[c] = r;
-        const bool f = r == (int32_t)c && p.cell_status[c] != 0;
+        p.uf[c] = r[k];
+        const bool f = r[k] == (int32_t)c && p.cell_status[c] != 0;
         flags |= (uint32_t)f << k;
         cnt += f;
       }
@@ -471,15 +499,9 @@ cudaError_t launch_core(const Plan& p, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-// Resets the pair lists between rings.
-__global__ void k_pairs_reset(Plan p) {
-  if (threadIdx.x == 0) { p.desc->p_count = 0; p.desc->d_count = 0; }
-}
-
 cudaError_t launch_union(const Plan& p, cudaStream_t s) {
   for (int ring = 0; ring < 2; ++ring) {
     if (ring == 1) k_flatten<<<p.num_sms * 8, 256, 0, s>>>(p);
-    k_pairs_reset<<<1, 32, 0, s>>>(p);
     k_pairs<<<p.num_sms * 8, 256, 0, s>>>(p, ring, ring);
     k_pair_scan<<<p.num_sms * 8, 256, 0, s>>>(p);
     k_pair_warp<<<p.num_sms * 8, 256, 0, s>>>(p);
