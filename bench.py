@@ -222,7 +222,8 @@ def max_over_ranks(v: float, world: int) -> float:
     if world == 1:
         return v
     import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -345,6 +346,8 @@ def run_ours(args, world, rank, local):
             out["batched"] = run_batched(dev, args.batched_clouds)
         if args.serve_seconds > 0:
             out["serving"] = run_serving(dev, args.serve_seconds)
+    elif args.batched_clouds > 0:
+        out["batched"] = run_batched_sharded(dev, args.batched_clouds, world, rank)
     return out
 
 
@@ -358,16 +361,43 @@ def _ev_ms(fn):
     return a.elapsed_time(b), out
 
 
+def batch_config(n_clouds: int):
+    """Sizes (log-uniform in [256, 262144]), eps_i in [0.2, 1.0] and
+    min_samples_i in {4..32} of the batched workload, seeded."""
+    rng = np.random.default_rng(0)
+    sizes = np.exp(rng.uniform(np.log(256), np.log(262_144), size=n_clouds)).astype(np.int64)
+    eps = rng.uniform(0.2, 1.0, size=n_clouds)
+    ms = rng.integers(4, 33, size=n_clouds)
+    return sizes, eps, ms
+
+
+def run_batched_sharded(dev, n_clouds: int, world: int, rank: int) -> dict:
+    """The batched workload split across ranks by shard_clouds (independent
+    clouds, no collective on the data path): each rank clusters its shard in
+    one batched run; the time is the max over ranks."""
+    from dbscan_torch import dbscan2d_batched, shard_clouds, synthetic
+    sizes, eps, ms = batch_config(n_clouds)
+    mine = shard_clouds(sizes, world)[rank]
+    X, off = synthetic.blobs_with_noise_device(sizes[mine], seed=rank, device=dev)
+    dbscan2d_batched(X, off, eps[mine], ms[mine])  # warm-up
+    tb = [_ev_ms(lambda: dbscan2d_batched(X, off, eps[mine], ms[mine]))[0] for _ in range(3)]
+    _C_check()
+    t = max_over_ranks(statistics.median(tb), world)
+    del X
+    torch.cuda.empty_cache()
+    return {"workload": f"{n_clouds} clouds sharded over {world} ranks (longest-first greedy by points)",
+            "clouds": n_clouds, "points": int(sizes.sum()), "batched_ms": round(t, 3),
+            "batched_clouds_per_s": round(n_clouds / (t * 1e-3), 1),
+            "batched_mpoints_per_s": round(int(sizes.sum()) / (t * 1e-3) / 1e6, 1)}
+
+
 def run_batched(dev, n_clouds: int) -> dict:
     """Config 3: n_clouds independent clouds (sizes log-uniform in [256, 262144],
     eps_i in [0.2, 1.0], min_samples_i in {4..32}) clustered by one batched
     pipeline run, against a loop of plain calls over the same device-resident
     clouds. Both timed with CUDA events; labels compared cloud by cloud."""
     from dbscan_torch import dbscan2d, dbscan2d_batched, synthetic
-    rng = np.random.default_rng(0)
-    sizes = np.exp(rng.uniform(np.log(256), np.log(262_144), size=n_clouds)).astype(np.int64)
-    eps = rng.uniform(0.2, 1.0, size=n_clouds)
-    ms = rng.integers(4, 33, size=n_clouds)
+    sizes, eps, ms = batch_config(n_clouds)
     X, off = synthetic.blobs_with_noise_device(sizes, seed=0, device=dev)
     offl = off.tolist()
     dbscan2d_batched(X, off, eps, ms)  # warm-up

@@ -57,7 +57,7 @@ ArrayLike2D = Union[np.ndarray, torch.Tensor]
 
 __all__ = [
     "dbscan2d", "dbscan2d_profile", "dbscan2d_batched", "DBSCAN", "ArrayLike2D",
-    "BatchedPlan", "DbscanServer", "footprint_bytes", "check_status",
+    "BatchedPlan", "DbscanServer", "footprint_bytes", "shard_clouds", "check_status",
 ]
 
 try:
@@ -146,3 +146,4 @@ class DBSCAN:
 
 from .batched import BatchedPlan  # noqa: E402  (needs _C)
 from .serve import DbscanServer, footprint_bytes  # noqa: E402  (needs _C)
+from .shard import shard_clouds  # noqa: E402
