@@ -147,6 +147,80 @@ torch::Tensor require_cuda_copy(const torch::Tensor& X) {
               /*non_blocking=*/X.is_pinned());
 }
 
+// ----------------------------------------------------------- graph replay
+// The plain call's launch sequence (21 kernels, no host read-back) is
+// recorded by stream capture on a side stream that never executes work, and
+// the recording updates one executable graph per device
+// (cudaGraphExecUpdate: the topology is the same for every n, only kernel
+// arguments and grid sizes change), which is then launched on the caller's
+// stream. Back-to-back kernels of a graph start with smaller gaps than 21
+// separate launches. The first call on a device runs directly (it sets the
+// lazy kernel attributes of the cooperative kernels outside any capture);
+// after any graph API failure the device falls back to direct launches.
+// DBSCAN_TORCH_GRAPHS=0 turns the replay off.
+struct PlainGraph {
+  cudaStream_t side = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  bool warmed = false;
+  bool broken = false;
+};
+std::mutex g_graph_mu;
+std::map<int, PlainGraph> g_graphs;
+
+bool graphs_enabled() {
+  static const bool on = [] {
+    const char* v = std::getenv("DBSCAN_TORCH_GRAPHS");
+    return !(v != nullptr && v[0] == '0');
+  }();
+  return on;
+}
+
+// Enqueues the plain pipeline on `stream` as one graph launch; false when the
+// graph path is not available (nothing enqueued then).
+bool launch_as_graph(int dev, const float* X, int64_t n, double eps, int64_t min_samples,
+                     int32_t* labels, void* ws, size_t bytes, cudaStream_t stream) {
+  std::lock_guard<std::mutex> lock(g_graph_mu);
+  PlainGraph& g = g_graphs[dev];
+  if (g.broken) return false;
+  if (!g.warmed) {
+    g.warmed = true;
+    return false;
+  }
+  auto fail = [&g]() {
+    cudaGetLastError();
+    g.broken = true;
+    return false;
+  };
+  if (g.side == nullptr && cudaStreamCreateWithFlags(&g.side, cudaStreamNonBlocking) != cudaSuccess)
+    return fail();
+  if (cudaStreamBeginCapture(g.side, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return fail();
+  const int rc = dbs_dbscan2d(X, n, eps, min_samples, labels, ws, bytes, g.side);
+  cudaGraph_t graph = nullptr;
+  const cudaError_t ec = cudaStreamEndCapture(g.side, &graph);
+  if (rc != DBS_OK || ec != cudaSuccess || graph == nullptr) {
+    if (graph != nullptr) cudaGraphDestroy(graph);
+    return fail();
+  }
+  bool ok = false;
+  if (g.exec != nullptr) {
+    cudaGraphExecUpdateResultInfo info;
+    ok = cudaGraphExecUpdate(g.exec, graph, &info) == cudaSuccess;
+    if (!ok) {
+      cudaGetLastError();
+      cudaGraphExecDestroy(g.exec);
+      g.exec = nullptr;
+    }
+  }
+  if (!ok) ok = cudaGraphInstantiate(&g.exec, graph, 0) == cudaSuccess;
+  cudaGraphDestroy(graph);
+  if (!ok) {
+    g.exec = nullptr;
+    return fail();
+  }
+  if (cudaGraphLaunch(g.exec, stream) != cudaSuccess) return fail();
+  return true;
+}
+
 // Runs the plain pipeline on a contiguous CUDA tensor.
 torch::Tensor run_cuda(const torch::Tensor& Xc, double eps, int64_t min_samples) {
   c10::cuda::CUDAGuard guard(Xc.device());
@@ -157,9 +231,13 @@ torch::Tensor run_cuda(const torch::Tensor& Xc, double eps, int64_t min_samples)
   const size_t bytes = dbs_workspace_bytes(n, 1);
   auto ws = alloc_ws(bytes, Xc.device());
   cudaStream_t stream = at::cuda::getCurrentCUDAStream();
-  check_rc(dbs_dbscan2d(Xc.data_ptr<float>(), n, eps, min_samples, labels.data_ptr<int32_t>(),
-                        ws.data_ptr(), bytes, stream),
-           "dbscan2d");
+  const bool graphed = graphs_enabled() && !capturing(stream) &&
+                       launch_as_graph(Xc.device().index(), Xc.data_ptr<float>(), n, eps, min_samples,
+                                       labels.data_ptr<int32_t>(), ws.data_ptr(), bytes, stream);
+  if (!graphed)
+    check_rc(dbs_dbscan2d(Xc.data_ptr<float>(), n, eps, min_samples, labels.data_ptr<int32_t>(),
+                          ws.data_ptr(), bytes, stream),
+             "dbscan2d");
   after_launch(ws, stream);
   return labels;
 }

@@ -87,3 +87,18 @@ def test_labels_match_reference_cuda(name, X, eps, ms):
     ours = dbscan2d(torch.from_numpy(X).cuda(), eps, ms).cpu().numpy()
     diff = np.flatnonzero(ours != want)
     assert diff.size == 0, f"{name}: {diff.size} labels differ from the reference CUDA path"
+
+
+def test_graph_replay_across_sizes():
+    """Plain calls on CUDA tensors replay one cached graph per device, updated
+    call by call (new pointers, new grid sizes). Alternating sizes, and a
+    sparse cloud (radix path) between dense ones, keep the oracle's labels."""
+    rng = np.random.default_rng(21)
+    clouds = []
+    for n in (1, 5, 1000, 50_000, 3, 200_000, 700):
+        clouds.append(datasets.three_blobs(n) if n >= 10 else rng.normal(0, 1, (n, 2)).astype(np.float32))
+    sparse = rng.uniform(-3000, 3000, size=(20_000, 2)).astype(np.float32)
+    seq = clouds + [sparse] + clouds[::-1]
+    for X in seq:
+        got = dbscan2d(torch.from_numpy(X).cuda(), 0.5, 4).cpu().numpy()
+        assert np.array_equal(got, oracle.dbscan2d(X, 0.5, 4)), X.shape
