@@ -65,9 +65,10 @@ size_t carve(int64_t n, int32_t nseg, char* base, Plan* p) {
   q.cid = cv.take<int32_t>(N);
   q.qlist = cv.take<uint32_t>(N);
   q.blist = cv.take<uint32_t>(N);
-  // Candidate pairs (c, nc > c) of one ring: each unordered neighbour pair
-  // is listed once, so at most 4 per cell in ring 1 and 8 in ring 2.
-  q.pair_cap = 8 * (int64_t)N;
+  // Candidate pairs (c, nc > c) of one union pass: each unordered neighbour
+  // pair is listed once, so at most 2 per cell in pass 0 (4 side
+  // neighbours) and 10 in pass 1 (20 diagonal and outer neighbours).
+  q.pair_cap = 10 * (int64_t)N;
   q.plist = cv.take<int2>((size_t)q.pair_cap);
   q.dlist = cv.take<uint32_t>((size_t)q.pair_cap);
   q.dense_cap = kDenseFactor * (int64_t)N + kDenseSlack * (int64_t)nseg;

@@ -206,17 +206,23 @@ __device__ __forceinline__ bool pair_scan(const Plan& p, int32_t c0, int32_t c1,
 // worst case).
 constexpr int32_t kPairBudget = 96;
 
-// Stencil offsets (off = (dx+2)*5 + (dy+2)) of ring 1 (|dx|, |dy| <= 1) and
-// ring 2, centre excluded.
-__constant__ int8_t kRingOffs[2][16] = {
-    {6, 7, 8, 11, 13, 16, 17, 18, 0, 0, 0, 0, 0, 0, 0, 0},
-    {0, 1, 2, 3, 4, 5, 9, 10, 14, 15, 19, 20, 21, 22, 23, 24}};
+// Stencil offsets (off = (dx+2)*5 + (dy+2)) of the two passes, centre
+// excluded: pass 0 the four side neighbours; pass 1 the four diagonal
+// neighbours and the outer ring of the 5x5 stencil. A diagonal pair needs
+// many tests before a close pair turns up (the close points sit near one
+// shared corner), but in dense regions it is nearly always joined already
+// through the two side neighbours, so after pass 0 and a flatten it is
+// dropped without a scan.
+constexpr int kPassOffs = 20;
+__constant__ int8_t kRingOffs[2][kPassOffs] = {
+    {7, 11, 13, 17, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0},
+    {6, 8, 16, 18, 0, 1, 2, 3, 4, 5, 9, 10, 14, 15, 19, 20, 21, 22, 23, 24}};
 
-// Edges of the cell graph, in three compacted steps per ring (ring 1 =
-// |dx|, |dy| <= 1; ring 2 = the rest of the 5x5 stencil, run after a
-// flatten so that most of its pairs are already connected):
+// Edges of the cell graph, in three compacted steps per pass (pass 0 = side
+// neighbours; pass 1 = diagonal and outer neighbours, run after a flatten so
+// that most of its pairs are already connected):
 //   k_pairs       one thread per core cell: its neighbours nc > c of the
-//                 ring that are core cells and pass the box-box prune
+//                 pass that are core cells and pass the box-box prune
 //                 (dbscan_cuda.cu:329-351); with `skip_united` (after a
 //                 flatten) pairs already in one component are dropped.
 //                 Survivors go to a pair list.
@@ -232,7 +238,7 @@ __constant__ int8_t kRingOffs[2][16] = {
 __global__ void __launch_bounds__(256) k_pairs(Plan p, int ring, int skip_united) {
   Desc* d = p.desc;
   const uint32_t C = d->num_cells;
-  const int nofs = ring == 0 ? 8 : 16;
+  const int nofs = ring == 0 ? 4 : kPassOffs;
   const uint32_t stride = gridDim.x * blockDim.x;
   for (uint32_t base = blockIdx.x * blockDim.x; base < C; base += stride) {
     const uint32_t c = base + threadIdx.x;
@@ -243,7 +249,7 @@ __global__ void __launch_bounds__(256) k_pairs(Plan p, int ring, int skip_united
       const float4 bb_c = p.bbox[c];
       int32_t root_c = -1;
 #pragma unroll
-      for (int k = 0; k < 16; ++k) {
+      for (int k = 0; k < kPassOffs; ++k) {
         if (k >= nofs) continue;
         const int32_t nb = row[kRingOffs[ring][k]];
         if (nb <= (int32_t)c || p.cell_status[nb] == 0) continue;
@@ -330,9 +336,9 @@ __global__ void __launch_bounds__(256) k_pair_warp(Plan p) {
 // Point every cell at its current root (read-only walks: a concurrent
 // writer of uf[c] only ever stores an ancestor of c, so walks still end at
 // the root).
-// Between the rings: every cell to its root (so a find in ring 2's pair
-// listing is one load), and the pair lists emptied for ring 2 (ring 1 starts
-// from the counters k_init cleared; ring 1's k_pair_warp, which reads them,
+// Between the passes: every cell to its root (so a find in pass 1's pair
+// listing is one load), and the pair lists emptied for pass 1 (pass 0 starts
+// from the counters k_init cleared; pass 0's k_pair_warp, which reads them,
 // has finished when this kernel runs).
 __global__ void __launch_bounds__(256) k_flatten(Plan p) {
   Desc* d = p.desc;
