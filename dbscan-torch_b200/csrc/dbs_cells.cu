@@ -167,7 +167,7 @@ __device__ __forceinline__ void append_list(uint32_t* list, uint32_t* count, boo
 //     coalesced;
 //   - the 25-entry neighbour row of each cell, staged in shared memory and
 //     written as one contiguous block per warp.
-__global__ void __launch_bounds__(kCellThreads) k_cell_prep(Plan p) {
+__global__ void __launch_bounds__(kCellThreads, 5) k_cell_prep(Plan p) {
   __shared__ int32_t s_row[kCellThreads / 32][32 * kNgh];
   const uint32_t full = 0xffffffffu;
   const uint32_t lane = lane_id();
@@ -267,7 +267,7 @@ __global__ void __launch_bounds__(kCellThreads) k_cell_prep(Plan p) {
 
     // Neighbour row, off = (dx+2)*5 + (dy+2) as in the reference.
     if (valid) {
-      const SegInfo& g = p.seg_info[seg];
+      const SegInfo g = p.seg_info[seg];  // in registers for the 25 lookups
       const uint64_t local = p.cell_key[c] - g.base;
       const uint64_t gx = local >> g.ysh;
       const uint64_t gy = local & ((1ull << g.ysh) - 1ull);
@@ -277,14 +277,29 @@ __global__ void __launch_bounds__(kCellThreads) k_cell_prep(Plan p) {
 #pragma unroll
       for (int dy = 0; dy < 5; ++dy)
         ngy[dy] = compact_axis((int32_t)((uint32_t)ky + (uint32_t)(dy - 2)), g.by, g.py);
+      if (g.map_base >= 0) {
+        // Dense cloud: five map rows, 25 independent loads.
+        int32_t r[25];
 #pragma unroll
-      for (int dx = 0; dx < 5; ++dx) {
-        const uint64_t ngx = compact_axis((int32_t)((uint32_t)kx + (uint32_t)(dx - 2)), g.bx, g.px);
+        for (int dx = 0; dx < 5; ++dx) {
+          const uint64_t ngx = compact_axis((int32_t)((uint32_t)kx + (uint32_t)(dx - 2)), g.bx, g.px);
+          const int32_t* mrow = p.cell_map + g.map_base + (int64_t)(ngx << g.ysh);
 #pragma unroll
-        for (int dy = 0; dy < 5; ++dy) {
-          int32_t r = -1;
-          if (ngx != ~0ull && ngy[dy] != ~0ull) r = find_cell(p, g, seg, ngx, ngy[dy], C);
-          srow[lane * kNgh + dx * 5 + dy] = r;
+          for (int dy = 0; dy < 5; ++dy)
+            r[dx * 5 + dy] = (ngx != ~0ull && ngy[dy] != ~0ull) ? mrow[ngy[dy]] : -1;
+        }
+#pragma unroll
+        for (int k = 0; k < 25; ++k) srow[lane * kNgh + k] = r[k];
+      } else {
+#pragma unroll
+        for (int dx = 0; dx < 5; ++dx) {
+          const uint64_t ngx = compact_axis((int32_t)((uint32_t)kx + (uint32_t)(dx - 2)), g.bx, g.px);
+#pragma unroll
+          for (int dy = 0; dy < 5; ++dy) {
+            int32_t r = -1;
+            if (ngx != ~0ull && ngy[dy] != ~0ull) r = find_cell(p, g, seg, ngx, ngy[dy], C);
+            srow[lane * kNgh + dx * 5 + dy] = r;
+          }
         }
       }
     }

@@ -34,6 +34,12 @@ __device__ __forceinline__ void append(uint32_t* list, uint32_t* count, bool tak
   if (take) list[base + __popc(m & lanemask_lt())] = v;
 }
 
+// The 24 stencil offsets (off = (dx+2)*5 + (dy+2)) without the centre, the
+// nearest cells first: sides, diagonals, (+-2, 0) / (0, +-2), (+-1, +-2) /
+// (+-2, +-1), corners.
+__constant__ int8_t kNearFirst[24] = {7, 11, 13, 17, 6, 8, 16, 18, 2, 10, 14, 22,
+                                      1, 3, 5, 9, 15, 19, 21, 23, 0, 4, 20, 24};
+
 // Core flag of every query point, one thread per query. A query counts its
 // own cell wholesale (the reference never distance-tests the centre cell,
 // :231-233) plus the points within eps of the other 24 stencil cells that
@@ -57,11 +63,11 @@ __global__ void __launch_bounds__(kCellThreads) k_core(Plan p) {
       int32_t cnt = st1 - st0;
       const float2 q = p.xy[i];
       const int32_t* row = p.ngh + (int64_t)c * kNgh;
-      // A neighbour cell wholly within eps of q (point_box_max_d2) counts all
-      // its points without distance tests: the same count.
-      for (int off = 0; off < kNgh && cnt < ms; ++off) {
-        if (off == 12) continue;
-        const int32_t nb = row[off];
+      // Nearest cells first, so the count reaches ms (and stops) sooner; a
+      // neighbour cell wholly within eps of q (point_box_max_d2) counts all
+      // its points without distance tests. Neither changes the core flag.
+      for (int o = 0; o < kNgh - 1 && cnt < ms; ++o) {
+        const int32_t nb = row[kNearFirst[o]];
         if (nb < 0) continue;
         const float4 bb = p.bbox[nb];
         if (!(point_box_d2(q.x, q.y, bb) <= eps_sq)) continue;
