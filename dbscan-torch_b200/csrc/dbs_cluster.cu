@@ -478,10 +478,16 @@ __global__ void __launch_bounds__(kCellThreads) k_labels(Plan p) {
       const int32_t* row = p.ngh + (int64_t)c * kNgh;
       unsigned long long best = ~0ull;
       int32_t best_nb = -1;
-      for (int off = 0; off < kNgh; ++off) {
-        const int32_t nb = row[off];
+      float best_d2 = eps_sq;  // no candidate beyond this (eps, then the best so far)
+      // Centre cell, then nearest cells first. A cell whose box is farther
+      // than the best d2 found so far cannot hold a smaller (d2, index) key:
+      // its points are all strictly farther (point_box_d2 is a lower bound of
+      // their rounded d2). A box at exactly the best d2 is still scanned, for
+      // a tie with a smaller index.
+      for (int o = -1; o < kNgh - 1; ++o) {
+        const int32_t nb = row[o < 0 ? 12 : kNearFirst[o]];
         if (nb < 0 || p.cell_status[nb] == 0) continue;
-        if (!(point_box_d2(q.x, q.y, p.bbox[nb]) <= eps_sq)) continue;
+        if (!(point_box_d2(q.x, q.y, p.bbox[nb]) <= best_d2)) continue;
         const int32_t j1 = p.cell_start[nb + 1];
         for (int32_t j = p.cell_start[nb]; j < j1; ++j) {
           if (!p.is_core[j]) continue;
@@ -490,7 +496,7 @@ __global__ void __launch_bounds__(kCellThreads) k_labels(Plan p) {
           if (d2 <= eps_sq) {
             // d2 >= +0 and not NaN here, so its bits order like its value.
             const unsigned long long key = ((unsigned long long)__float_as_uint(d2) << 32) | p.perm[j];
-            if (key < best) { best = key; best_nb = nb; }
+            if (key < best) { best = key; best_nb = nb; best_d2 = d2; }
           }
         }
       }
