@@ -54,18 +54,19 @@ EPS, MIN_SAMPLES = 0.5, 10
 WORKLOAD = "constant_density_10M"
 L2_FLUSH_BYTES = 512 << 20
 # Kernel launches of one dbscan2d call (tests/test_launch_count.py counts them
-# with the profiler): init, bounds, seg_finalize | csort, keys, radix | rle |
-# cell_prep, huge_bbox | core, status | 2 x (pairs, pair_scan, pair_warp) +
-# flatten | ids, cid | labels. Kernels whose work the
-# device-side plan skips (radix passes under the counting sort, the huge-cell
-# pass without huge cells) still launch and return at once.
-KERNELS_PER_CALL = 21
+# with the profiler): init, bounds, seg_finalize | csort_clear, csort_count,
+# csort, keys, radix | rle | cell_prep, huge_bbox | core, status |
+# 2 x (pairs, pair_scan, pair_warp) + flatten | ids, cid | labels. Kernels
+# whose work the device-side plan skips (radix passes under the counting
+# sort, the huge-cell pass without huge cells) still launch and return at once.
+KERNELS_PER_CALL = 23
 # Launches per reference stage (the profile entry point times stages).
-STAGE_LAUNCHES = {"cell_keys": 3, "sort_gather": 3, "boundary_scan": 1, "build_ngh": 2,
+STAGE_LAUNCHES = {"cell_keys": 3, "sort_gather": 5, "boundary_scan": 1, "build_ngh": 2,
                   "core_mark": 2, "union_find": 7, "cluster_id": 2, "border_assign": 1}
-# The kernel that does a stage's work when one kernel does (the others of the
-# stage return at once on this workload).
-STAGE_KERNEL = {"sort_gather": "k_csort", "build_ngh": "k_cell_prep", "border_assign": "k_labels"}
+# The kernels that do a stage's work on this workload (the others of the
+# stage return at once).
+STAGE_KERNEL = {"sort_gather": ("k_csort_clear", "k_csort_count", "k_csort"),
+                "build_ngh": ("k_cell_prep",), "border_assign": ("k_labels",)}
 PROFILE_MD = os.path.join(ROOT, "profiles", "kernels_constant_density_10M.md")
 
 
@@ -150,18 +151,22 @@ def stage_bytes(n: int, cells: int, passes: int, kb: int) -> dict:
     }
 
 
-def ncu_traffic(kernel: str):
-    """DRAM bytes (read + write) per launch of `kernel` from the committed ncu
-    summary of this workload (its table gives MB read and written)."""
+def ncu_traffic(kernels):
+    """DRAM bytes (read + write) of one launch of each of `kernels`, summed,
+    from the committed ncu summary of this workload (its table gives MB read
+    and written per kernel); None unless every kernel has a row."""
+    found = {}
     try:
         with open(PROFILE_MD) as f:
             for line in f:
                 cols = [c.strip() for c in line.strip().strip("|").split("|")]
-                if len(cols) > 3 and cols[0] == kernel:
-                    return int(round((float(cols[2]) + float(cols[3])) * 1e6))
+                if len(cols) > 3 and cols[0] in kernels and cols[0] not in found:
+                    found[cols[0]] = (float(cols[2]) + float(cols[3])) * 1e6
     except (OSError, ValueError):
-        pass
-    return None
+        return None
+    if len(found) != len(kernels):
+        return None
+    return int(round(sum(found.values())))
 
 
 def cpu_baseline(X: np.ndarray, eps: float, ms: int, budget_s: float = 15.0):
@@ -288,17 +293,18 @@ def run_ours(args, world, rank, local):
     cells, passes, kb = info["num_cells"], info["passes"], info["key_bytes"]
     sb = stage_bytes(N_POINTS, cells, passes, kb)
     dom = max(STAGE_LAUNCHES, key=lambda s: prof[s])
-    kernel = STAGE_KERNEL.get(dom, dom) if (dom != "sort_gather" or passes == 0) else "k_radix"
+    kernels = STAGE_KERNEL.get(dom, (dom,)) if (dom != "sort_gather" or passes == 0) else ("k_keys", "k_radix")
+    kernel = "+".join(kernels)
     peak, peak_kind = _peaks()
-    # One launch of the stage's kernel does the stage's work; the stage time
-    # also holds the launches that return at once (a few microseconds).
+    # The stage's kernels (one launch each) do its work; the stage time also
+    # holds the launches that return at once (a few microseconds).
     achieved = sb[dom] / (prof[dom] * 1e-3) / 1e9
     b_alg_total = sum(sb.values())
     roof = {"bound": "hbm", "kernel": kernel, "stage": dom, "launches": STAGE_LAUNCHES[dom],
             "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "peak_source": peak_kind,
             "alg_bytes_per_launch": sb[dom],
-            "traffic": ncu_traffic(kernel) if dom in STAGE_KERNEL else None,
+            "traffic": ncu_traffic(kernels) if dom in STAGE_KERNEL else None,
             "pipeline_alg_bytes": b_alg_total,
             "pipeline_frac": round(b_alg_total / (ms_mean * 1e-3) / 1e9 / peak, 4),
             "stage_ms": {s: round(v, 4) for s, v in prof.items()},
