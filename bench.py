@@ -17,6 +17,9 @@ synthetic data. One step = one dbscan2d call over the whole cloud.
   cpu_baseline  the reference's own CPU implementation (built from its
             sources into oracle/_ref/cpu) on the box's host cores, timed on
             the same workload
+  configs   the other plain-call workloads on the device: 100k blobs with
+            noise, constant density at 1M and 5M, the adversarial 4M cloud
+            (min_samples 4 and 32) (--no-configs skips them)
   batched   4,096 clouds (sizes log-uniform in [256, 262144]) in one batched
             pipeline run vs a loop of plain calls: clouds/s of each
             (--batched-clouds; 0 skips)
@@ -348,6 +351,8 @@ def run_ours(args, world, rank, local):
     del labels, X, flush, X_host
     torch.cuda.empty_cache()
     if world == 1:
+        if not args.no_configs:
+            out["configs"] = run_configs(dev)
         if args.batched_clouds > 0:
             out["batched"] = run_batched(dev, args.batched_clouds)
         if args.serve_seconds > 0:
@@ -432,6 +437,34 @@ def run_batched(dev, n_clouds: int) -> dict:
             "speedup": round(tp / t_b, 2), "labels_equal": bool(equal)}
 
 
+def run_configs(dev) -> dict:
+    """The other plain-call workloads, device-resident, CUDA events around each
+    call (median of 7 after 3 warm-ups): config 0 (100k blobs with noise),
+    config 1 at 1M and 5M points, config 2 (adversarial 4M cloud, min_samples
+    4 and 32)."""
+    from dbscan_torch import dbscan2d, synthetic
+    cases = [("blobs_100k", lambda: synthetic.blobs_with_noise(100_000, seed=0), 0.5, 10),
+             ("constant_density_1M", lambda: synthetic.constant_density(1_000_000, seed=0), 0.5, 10),
+             ("constant_density_5M", lambda: synthetic.constant_density(5_000_000, seed=0), 0.5, 10),
+             ("adversarial_4M_ms4", lambda: synthetic.adversarial(4_000_000, seed=0), 0.5, 4),
+             ("adversarial_4M_ms32", None, 0.5, 32)]
+    out = {}
+    X = None
+    for name, gen, eps, ms in cases:
+        if gen is not None:
+            X = torch.from_numpy(gen()).to(dev)
+        for _ in range(3):
+            dbscan2d(X, eps, ms)
+        ts = [_ev_ms(lambda: dbscan2d(X, eps, ms))[0] for _ in range(7)]
+        t = statistics.median(ts)
+        out[name] = {"n_points": int(X.shape[0]), "eps": eps, "min_samples": ms, "ms": round(t, 4),
+                     "mpoints_per_s": round(X.shape[0] / (t * 1e-3) / 1e6, 1)}
+    _C_check()
+    del X
+    torch.cuda.empty_cache()
+    return out
+
+
 def _C_check():
     from dbscan_torch import check_status
     check_status()
@@ -509,6 +542,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the timings of the other plain-call workloads")
     ap.add_argument("--batched-clouds", type=int, default=4096,
                     help="clouds of the batched comparison (0 skips it)")
     ap.add_argument("--serve-seconds", type=float, default=10.0,
