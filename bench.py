@@ -41,7 +41,6 @@ import os
 import statistics
 import subprocess
 import sys
-import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -83,39 +82,70 @@ def _peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+    """nvidia-smi clocks / throttle reasons sampled during the timed region:
+    one `nvidia-smi -lms 5` child started (and its first sample awaited)
+    before timing begins, writing timestamped lines to a file -- no process
+    is forked while the timed steps run -- and stopped afterwards (by its own
+    PID). Only the samples stamped inside the timed window are summarised
+    (the nearest ones when the window is shorter than the sampling period)."""
 
-    FIELDS = ("clocks.sm,clocks.max.sm,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+    FIELDS = ("timestamp,clocks.sm,clocks.max.sm,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
               "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
               "clocks_event_reasons.sw_power_cap")
 
     def __init__(self, index: int):
         self.index = index
         self.samples = []
-        self._stop = threading.Event()
-        self._t = None
-
-    def _run(self):
-        while not self._stop.is_set():
-            try:
-                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
-                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
-                                     timeout=5).stdout.strip()
-                if out:
-                    self.samples.append([v.strip() for v in out.split(",")])
-            except Exception:
-                pass
-            self._stop.wait(0.2)
+        self._proc = None
+        self._file = None
 
     def __enter__(self):
-        self._t = threading.Thread(target=self._run, daemon=True)
-        self._t.start()
+        import tempfile
+        self._file = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
+        try:
+            self._proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "5"],
+                stdout=self._file, stderr=subprocess.DEVNULL)
+            t_end = time.time() + 3.0
+            while time.time() < t_end and os.path.getsize(self._file.name) == 0:
+                time.sleep(0.02)
+        except Exception:
+            self._proc = None
+        self._t0 = time.time()
         return self
 
     def __exit__(self, *a):
-        self._stop.set()
-        if self._t:
-            self._t.join(timeout=10)
+        self._t1 = time.time()
+        if self._proc is not None:
+            time.sleep(0.05)  # the samples of the last timed steps
+            self._proc.terminate()
+            try:
+                self._proc.wait(timeout=5)
+            except Exception:
+                self._proc.kill()
+        import datetime
+        rows = []
+        try:
+            with open(self._file.name) as f:
+                for line in f:
+                    v = [x.strip() for x in line.split(",")]
+                    if len(v) < 8:
+                        continue
+                    try:
+                        ts = datetime.datetime.strptime(v[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                    except ValueError:
+                        ts = None
+                    rows.append((ts, v[1:]))
+            os.unlink(self._file.name)
+        except Exception:
+            pass
+        inside = [r for t, r in rows if t is not None and self._t0 <= t <= self._t1]
+        if not inside and rows:  # window shorter than the sampling period
+            mid = (self._t0 + self._t1) / 2
+            timed = [(abs(t - mid), r) for t, r in rows if t is not None]
+            inside = [min(timed, key=lambda x: x[0])[1]] if timed else [rows[-1][1]]
+        self.samples = inside
 
     def summary(self):
         if not self.samples:
@@ -126,7 +156,8 @@ class ClockSampler:
         reasons = sorted({names[k] for s in self.samples for k in range(4)
                           if len(s) > 3 + k and s[3 + k].lower().startswith("active")})
         return {"sm_mhz": statistics.median(sm) if sm else None,
-                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons}
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.samples)}
 
 
 def stage_bytes(n: int, cells: int, passes: int, kb: int) -> dict:
@@ -264,8 +295,12 @@ def run_ours(args, world, rank, local):
 
     # Shape of the pipeline on this input (cells, key width, passes).
     _, info = _C.dbscan2d_info(X, EPS, MIN_SAMPLES)
+    # Warm-up as the timed loop runs: each result held until the next call
+    # returns, so both label buffers the loop alternates between have their
+    # launch graph recorded before timing starts.
+    labels = None
     for _ in range(max(3, args.warmup)):
-        dbscan2d(X, EPS, MIN_SAMPLES)
+        labels = dbscan2d(X, EPS, MIN_SAMPLES)
     _C.check_status()
 
     barrier(world)
@@ -282,6 +317,8 @@ def run_ours(args, world, rank, local):
     barrier(world)
     _C.check_status()
     step_ms = [a.elapsed_time(b) for a, b in ev]
+    step_stats = {"min": round(min(step_ms), 4), "median": round(statistics.median(step_ms), 4),
+                  "max": round(max(step_ms), 4)}
     ms_mean = sum(step_ms) / len(step_ms)
     ms_max = max_over_ranks(ms_mean, world)
     value = world * N_POINTS / (ms_max * 1e-3) / 1e6
@@ -334,6 +371,7 @@ def run_ours(args, world, rank, local):
 
     out = {"metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max, 4),
+           "step_ms": step_stats,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
            "data": "synthetic (seeded constant-density Gaussian blobs + 2% noise)",
            "config": {"workload": WORKLOAD, "n_points": N_POINTS, "eps": EPS,

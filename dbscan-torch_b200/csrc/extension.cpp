@@ -148,19 +148,42 @@ torch::Tensor require_cuda_copy(const torch::Tensor& X) {
 }
 
 // ----------------------------------------------------------- graph replay
-// The plain call's launch sequence (21 kernels, no host read-back) is
-// recorded by stream capture on a side stream that never executes work, and
-// the recording updates one executable graph per device
-// (cudaGraphExecUpdate: the topology is the same for every n, only kernel
-// arguments and grid sizes change), which is then launched on the caller's
-// stream. Back-to-back kernels of a graph start with smaller gaps than 21
-// separate launches. The first call on a device runs directly (it sets the
-// lazy kernel attributes of the cooperative kernels outside any capture);
-// after any graph API failure the device falls back to direct launches.
-// DBSCAN_TORCH_GRAPHS=0 turns the replay off.
+// The plain call's launch sequence (21+ kernels, no host read-back) is
+// replayed as a CUDA graph. Each device keeps a few executable graphs keyed
+// by the exact call (input, label and workspace pointers, n, eps,
+// min_samples): a repeated call -- the same buffers, or a loop alternating
+// between two label buffers -- costs one graph launch. Any other call is
+// recorded by stream capture on a side stream that never executes work and
+// updates the least recently used executable graph (cudaGraphExecUpdate: the
+// topology is the same for every n, only kernel arguments and grid sizes
+// change), which is then launched on the caller's stream. The first call on
+// a device runs directly (it sets the lazy kernel attributes of the
+// cooperative kernels outside any capture); after any graph API failure the
+// device falls back to direct launches. DBSCAN_TORCH_GRAPHS=0 turns the
+// replay off.
+struct GraphKey {
+  const void* X;
+  int64_t n;
+  double eps;
+  int64_t min_samples;
+  void* labels;
+  void* ws;
+  size_t bytes;
+  bool operator==(const GraphKey& o) const {
+    return X == o.X && n == o.n && eps == o.eps && min_samples == o.min_samples &&
+           labels == o.labels && ws == o.ws && bytes == o.bytes;
+  }
+};
+struct GraphEntry {
+  GraphKey key{};
+  cudaGraphExec_t exec = nullptr;
+  uint64_t used = 0;
+};
+constexpr int kGraphEntries = 4;
 struct PlainGraph {
   cudaStream_t side = nullptr;
-  cudaGraphExec_t exec = nullptr;
+  GraphEntry entries[kGraphEntries];
+  uint64_t clock = 0;
   bool warmed = false;
   bool broken = false;
 };
@@ -191,33 +214,45 @@ bool launch_as_graph(int dev, const float* X, int64_t n, double eps, int64_t min
     g.broken = true;
     return false;
   };
-  if (g.side == nullptr && cudaStreamCreateWithFlags(&g.side, cudaStreamNonBlocking) != cudaSuccess)
-    return fail();
-  if (cudaStreamBeginCapture(g.side, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return fail();
-  const int rc = dbs_dbscan2d(X, n, eps, min_samples, labels, ws, bytes, g.side);
-  cudaGraph_t graph = nullptr;
-  const cudaError_t ec = cudaStreamEndCapture(g.side, &graph);
-  if (rc != DBS_OK || ec != cudaSuccess || graph == nullptr) {
-    if (graph != nullptr) cudaGraphDestroy(graph);
-    return fail();
+  const GraphKey key{X, n, eps, min_samples, labels, ws, bytes};
+  GraphEntry* hit = nullptr;
+  GraphEntry* victim = &g.entries[0];
+  for (GraphEntry& e : g.entries) {
+    if (e.exec != nullptr && e.key == key) { hit = &e; break; }
+    if (e.exec == nullptr || (victim->exec != nullptr && e.used < victim->used)) victim = &e;
   }
-  bool ok = false;
-  if (g.exec != nullptr) {
-    cudaGraphExecUpdateResultInfo info;
-    ok = cudaGraphExecUpdate(g.exec, graph, &info) == cudaSuccess;
-    if (!ok) {
-      cudaGetLastError();
-      cudaGraphExecDestroy(g.exec);
-      g.exec = nullptr;
+  if (hit == nullptr) {
+    if (g.side == nullptr && cudaStreamCreateWithFlags(&g.side, cudaStreamNonBlocking) != cudaSuccess)
+      return fail();
+    if (cudaStreamBeginCapture(g.side, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return fail();
+    const int rc = dbs_dbscan2d(X, n, eps, min_samples, labels, ws, bytes, g.side);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(g.side, &graph);
+    if (rc != DBS_OK || ec != cudaSuccess || graph == nullptr) {
+      if (graph != nullptr) cudaGraphDestroy(graph);
+      return fail();
     }
+    bool ok = false;
+    if (victim->exec != nullptr) {
+      cudaGraphExecUpdateResultInfo info;
+      ok = cudaGraphExecUpdate(victim->exec, graph, &info) == cudaSuccess;
+      if (!ok) {
+        cudaGetLastError();
+        cudaGraphExecDestroy(victim->exec);
+        victim->exec = nullptr;
+      }
+    }
+    if (!ok) ok = cudaGraphInstantiate(&victim->exec, graph, 0) == cudaSuccess;
+    cudaGraphDestroy(graph);
+    if (!ok) {
+      victim->exec = nullptr;
+      return fail();
+    }
+    victim->key = key;
+    hit = victim;
   }
-  if (!ok) ok = cudaGraphInstantiate(&g.exec, graph, 0) == cudaSuccess;
-  cudaGraphDestroy(graph);
-  if (!ok) {
-    g.exec = nullptr;
-    return fail();
-  }
-  if (cudaGraphLaunch(g.exec, stream) != cudaSuccess) return fail();
+  hit->used = ++g.clock;
+  if (cudaGraphLaunch(hit->exec, stream) != cudaSuccess) return fail();
   return true;
 }
 
