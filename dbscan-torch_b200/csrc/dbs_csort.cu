@@ -5,8 +5,9 @@
 //   k_boundary_flags / inclusive_scan / k_extract_cell_start :84-120 and the
 //   host read of num_cells :612-617.
 //
-// When every cloud's compacted key range is dense (at most 4N + 4096 keys,
-// the same rule that gives a cloud a dense cell map), the sort needs no
+// When the compacted key range is dense (every cloud within 6N + 4096 keys,
+// or all clouds of a batch within that budget summed -- the rule that gives
+// clouds a dense cell map), the sort needs no
 // radix passes: a key *is* its bin. Two ordinary launches, then one
 // cooperative kernel with phases separated by grid barriers:
 //   0. clear the per-key counters (k_csort_clear)
@@ -189,6 +190,11 @@ __device__ __forceinline__ void scan_bins(const Plan& p, int64_t W, uint32_t* s_
     const bool one = p.nseg == 1;
     const uint64_t base0 = p.seg_info[0].base;
     uint32_t carry_cs = p.blk_sum[blockIdx.x], carry_ne = p.blk_ne[blockIdx.x];
+    // Cloud of each key: one search for the thread's first key, then a walk
+    // forward (a thread's keys only increase, so the walk covers each cloud
+    // boundary once; a search per key cost a binary search over every cloud
+    // for each of the 834M keys of a 4,096-cloud batch).
+    int32_t sg = one ? 0 : seg_of_key(p, (uint64_t)min(r0 + (int64_t)threadIdx.x * kI, W > 0 ? W - 1 : 0));
     for (int64_t cb = r0; cb < r1; cb += (int64_t)blockDim.x * kI) {
       const int64_t b0 = cb + (int64_t)threadIdx.x * kI;
       const bool full = b0 + kI <= r1;
@@ -216,7 +222,8 @@ __device__ __forceinline__ void scan_bins(const Plan& p, int64_t W, uint32_t* s_
         o[k] = off;
         m[k] = c[k] ? (int32_t)cell : -1;
         if (b < r1) {
-          const int32_t sg = one ? 0 : seg_of_key(p, (uint64_t)b);
+          if (!one)
+            while (sg + 1 < p.nseg && p.seg_info[sg + 1].base <= (uint64_t)b) ++sg;
           if ((uint64_t)b == (one ? base0 : p.seg_info[sg].base)) p.seg_info[sg].cell_begin = (int32_t)cell;
           if (c[k]) {
             p.cell_start[cell] = (int32_t)off;

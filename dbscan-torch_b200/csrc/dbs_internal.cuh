@@ -52,8 +52,10 @@ constexpr int32_t kHugeCell = 4096;   // cells whose box is reduced by many warp
 constexpr int32_t kHugeChunk = 2048;  // points per chunk of a huge cell
 
 // Dense cell map: a cloud whose compacted key range W satisfies
-// W <= kDenseFactor * N + kDenseSlack resolves neighbours with one load.
-constexpr int64_t kDenseFactor = 4;
+// W <= kDenseFactor * N + kDenseSlack resolves neighbours with one load; a
+// batch whose clouds' ranges fit the summed budget gets a map for every
+// cloud (k_seg_finalize).
+constexpr int64_t kDenseFactor = 6;
 constexpr int64_t kDenseSlack = 4096;
 
 // Error bits of Desc::status (OR-ed by kernels, read by the host).

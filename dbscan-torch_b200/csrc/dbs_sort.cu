@@ -257,6 +257,22 @@ __global__ void __launch_bounds__(1024) k_seg_finalize(Plan p) {
     }
     __syncthreads();
   }
+  // Pooled budget: when the key ranges of all clouds together fit the dense
+  // map (kDenseFactor * N + kDenseSlack per cloud, summed), every cloud gets
+  // its slice of the map -- a cloud sparser than its own share borrows from
+  // denser ones -- and the counting sort covers the whole batch: a cloud's
+  // global key then equals its map index (map_base = base).
+  __shared__ int s_pooled;
+  if (threadIdx.x == 0)
+    s_pooled = !p.force_radix && !s_overflow && s_carry_range <= (unsigned long long)p.dense_cap &&
+               s_carry_range < (1ull << 31);
+  __syncthreads();
+  if (s_pooled) {
+    for (int32_t s = threadIdx.x; s < p.nseg; s += blockDim.x) {
+      SegInfo& g = p.seg_info[s];
+      g.map_base = (int64_t)g.base;
+    }
+  }
   if (threadIdx.x == 0) {
     Desc* d = p.desc;
     // The last key is base[last] + range[last] - 1 (fits even when the sum
@@ -271,12 +287,14 @@ __global__ void __launch_bounds__(1024) k_seg_finalize(Plan p) {
     d->nbits = nbits;
     d->npasses = np < 1 ? 1 : np;
     d->key64 = nbits > 32 ? 1 : 0;
-    unsigned long long dt = s_carry_dense;
+    unsigned long long dt = s_pooled ? s_carry_range : s_carry_dense;
     if ((long long)dt > p.dense_cap) dt = 0;  // cannot happen by construction
     d->dense_total = dt;
-    // Counting sort when every non-empty cloud is dense (then the global key
-    // of a point is its dense-map index) and keys fit 31 bits.
-    d->dense_sort = (!p.force_radix && !s_sparse && !s_overflow && dt < (1ull << 31)) ? 1u : 0u;
+    // Counting sort when the pooled map covers every cloud, or every
+    // non-empty cloud is dense on its own (then the global key of a point is
+    // its dense-map index too), and keys fit 31 bits.
+    d->dense_sort = (s_pooled || (!p.force_radix && !s_sparse && !s_overflow && dt < (1ull << 31)))
+                        ? 1u : 0u;
     if (s_overflow) set_error(d, kErrKeySpace);
   }
 }

@@ -2,7 +2,7 @@
 (bit-exact labels).
 
 Points sit in W = wx * 2^ceil(log2 wy) compacted cell keys (cell side
-eps / sqrt(2)). A dense key space (W <= 4N + 4096) takes the counting sort
+eps / sqrt(2)). A dense key space (W <= 6N + 4096) takes the counting sort
 over keys, whose per-key counters, scan and dense cell map all scale with W;
 a sparse one takes the radix sort. The clouds below cover W from under a
 million keys to 18 million, a sparse key space, a cloud with most points in
@@ -38,7 +38,7 @@ FORMS = [
     ("dense_W1.5M", _rect(500_000, 1500, 1000, 2), 3, True),
     ("dense_W4.1M", _rect(1_200_000, 2000, 2000, 3), 3, True),
     ("dense_W18M", _rect(5_000_000, 4500, 4000, 4), 3, True),
-    ("radix_sparse", _rect(100_000, 3000, 3000, 5), 2, False),     # W ~ 12M > 4N + 4096
+    ("radix_sparse", _rect(100_000, 3000, 3000, 5), 2, False),     # W ~ 12M > 6N + 4096
     ("hot_cell", synthetic.adversarial(400_000, seed=6), 4, True),  # half the points in a few cells
 ]
 
@@ -54,6 +54,25 @@ def test_sort_form_matches_oracle(name, X, ms, dense):
     assert diff.size == 0, f"{name}: {diff.size}/{X.shape[0]} labels differ"
     # A second run on the same workspace layout gives the same labels.
     assert np.array_equal(dbscan2d(Xd, EPS, ms).cpu().numpy(), want)
+
+
+def test_batched_pooled_budget():
+    """A batch whose clouds are sparse on their own (key range above 6N + 4096
+    each) but fit the summed budget takes the counting sort over one pooled
+    map; labels per cloud equal plain calls (which take the radix sort)."""
+    rng = np.random.default_rng(9)
+    dense = [synthetic.constant_density(200_000, seed=k) for k in range(3)]
+    sparse = [rng.uniform(-40, 40, size=(300, 2)).astype(np.float32) for _ in range(5)]
+    clouds = dense[:1] + sparse[:2] + dense[1:] + sparse[2:]
+    X = np.concatenate(clouds)
+    off = np.concatenate([[0], np.cumsum([len(c) for c in clouds])])
+    Xd = torch.from_numpy(X).cuda()
+    lab = dbscan2d_batched(Xd, off.tolist(), 0.5, 4).cpu().numpy()
+    for k, c in enumerate(clouds):
+        want = oracle.dbscan2d(c, 0.5, 4)
+        assert np.array_equal(lab[off[k]:off[k + 1]], want), f"cloud {k}"
+        plain = dbscan2d(torch.from_numpy(c).cuda(), 0.5, 4).cpu().numpy()
+        assert np.array_equal(plain, want)
 
 
 def test_batched_dense_clouds():
