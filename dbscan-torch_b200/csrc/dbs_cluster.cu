@@ -462,16 +462,27 @@ __global__ void __launch_bounds__(256) k_cid(Plan p) {
 // core point within eps that minimises (d2, input index) over the 25
 // stencil cells with a core point, pruned by the point-box test, or -1.
 // Items after that are all sorted points; core ones take their cell's id.
+// Item order: with labels that fit L2 (n <= kCoreFirstPoints, 64 MB), the
+// border items go first so their uneven scans overlap the core items of
+// other warps (121 us against 136 us at 10M points); with more points the
+// core items go first, so the whole grid sweeps the sorted points -- and the
+// input-order label writes of the clouds there -- together instead of
+// scattering them over the whole label array (3.5 ms against 7.6 ms for a
+// 151M-point, 4,096-cloud batch).
+constexpr int64_t kCoreFirstPoints = 16 << 20;
+
 __global__ void __launch_bounds__(kCellThreads) k_labels(Plan p) {
   const int64_t n = p.n;
   const int64_t bn = p.desc->b_count;
   const int64_t total = bn + n;
+  const bool core_first = n > kCoreFirstPoints;
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
        t += (int64_t)gridDim.x * blockDim.x) {
     int64_t i;
     int32_t lab;
-    if (t < bn) {
-      i = p.blist[t];
+    const int64_t bt = core_first ? t - n : t;  // index into the border list
+    if (bt >= 0 && bt < bn) {
+      i = p.blist[bt];
       const int32_t c = p.point_cell[i];
       const float eps_sq = p.seg_param[p.cell_seg[c]].eps_sq;
       const float2 q = p.xy[i];
@@ -502,7 +513,7 @@ __global__ void __launch_bounds__(kCellThreads) k_labels(Plan p) {
       }
       lab = best_nb < 0 ? -1 : p.cid[best_nb];
     } else {
-      i = t - bn;
+      i = core_first ? t : t - bn;
       if (!p.is_core[i]) continue;
       lab = p.cid[p.point_cell[i]];
     }

@@ -118,3 +118,17 @@ def test_special_coordinates(kind):
     ref = refmod.load("cuda")
     if ref is not None:
         assert np.array_equal(ours, ref.dbscan2d(torch.from_numpy(X).cuda(), EPS, 5).cpu().numpy())
+
+
+def test_batched_above_core_first_threshold():
+    """More than 16M points in one run: the label pass orders its work core
+    labels first (the label array is larger than L2); labels still equal a
+    plain call per cloud."""
+    sizes = [4_500_000, 4_500_000, 4_500_000, 4_500_000]
+    X, off = synthetic.blobs_with_noise_device(sizes, seed=5, device="cuda")
+    offl = off.tolist()
+    eps, ms = [0.3, 0.5, 0.8, 1.0], [4, 10, 16, 32]
+    lab = dbscan2d_batched(X, offl, eps, ms)
+    for k in range(len(sizes)):
+        want = dbscan2d(X[offl[k]:offl[k + 1]], eps[k], ms[k])
+        assert torch.equal(lab[offl[k]:offl[k + 1]], want), f"cloud {k}"
