@@ -68,7 +68,9 @@ size_t carve(int64_t n, int32_t nseg, char* base, Plan* p) {
   // Candidate pairs (c, nc > c) of one union pass: each unordered neighbour
   // pair is listed once, so at most 2 per cell in pass 0 (4 side
   // neighbours) and 10 in pass 1 (20 diagonal and outer neighbours).
-  q.pair_cap = 10 * (int64_t)N;
+  // Entries are counted in 32 bits: at most 2^32 - 1 (reached only beyond
+  // 429M points; k_pairs reports an overflow in the status word).
+  q.pair_cap = std::min<int64_t>(10 * (int64_t)N, 0xffffffffLL);
   q.plist = cv.take<int2>((size_t)q.pair_cap);
   q.dlist = cv.take<uint32_t>((size_t)q.pair_cap);
   q.dense_cap = kDenseFactor * (int64_t)N + kDenseSlack * (int64_t)nseg;

@@ -279,7 +279,10 @@ __global__ void __launch_bounds__(256) k_pairs(Plan p, int ring, int skip_united
     }
     const uint32_t tot = __shfl_sync(kFull, x, 31);
     uint32_t at = 0;
-    if (lane_id() == 31 && tot) at = atomicAdd(&d->p_count, tot);
+    if (lane_id() == 31 && tot) {
+      at = atomicAdd(&d->p_count, tot);
+      if ((uint64_t)at + tot > (uint64_t)p.pair_cap) set_error(d, kErrCapacity);
+    }
     at = __shfl_sync(kFull, at, 31) + x - cnt;
     while (mask) {
       const int k = __ffs(mask) - 1;
@@ -292,12 +295,12 @@ __global__ void __launch_bounds__(256) k_pairs(Plan p, int ring, int skip_united
 
 __global__ void __launch_bounds__(256) k_pair_scan(Plan p) {
   Desc* d = p.desc;
-  const uint32_t np = min(d->p_count, (uint32_t)p.pair_cap);
-  const uint32_t stride = gridDim.x * blockDim.x;
-  for (uint32_t base = blockIdx.x * blockDim.x; base < np; base += stride) {
-    const uint32_t t = base + threadIdx.x;
+  const int64_t np = min((int64_t)d->p_count, p.pair_cap);
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < np; base += stride) {
+    const uint32_t t = (uint32_t)(base + threadIdx.x);
     bool deferred = false;
-    if (t < np) {
+    if ((int64_t)t < np) {
       const int2 pr = p.plist[t];
       const int32_t c = pr.x, nb = pr.y;
       const float eps_sq = p.seg_param[p.cell_seg[c]].eps_sq;
@@ -325,10 +328,10 @@ __global__ void __launch_bounds__(256) k_pair_scan(Plan p) {
 
 __global__ void __launch_bounds__(256) k_pair_warp(Plan p) {
   Desc* d = p.desc;
-  const uint32_t nd = d->d_count;
+  const int64_t nd = min((int64_t)d->d_count, p.pair_cap);
   const uint32_t lane = lane_id();
-  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < nd; w += nwarps) {
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < nd; w += nwarps) {
     const int2 pr = p.plist[p.dlist[w]];
     const int32_t c = pr.x, nb = pr.y;
     const float eps_sq = p.seg_param[p.cell_seg[c]].eps_sq;

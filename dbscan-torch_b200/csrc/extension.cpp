@@ -59,10 +59,21 @@ std::vector<PendingStatus> g_slots;
 size_t g_next = 0;
 constexpr size_t kSlots = 64;
 
+// What the device status bits of include/dbscan_b200.h mean.
+std::string status_text(uint32_t st) {
+  std::string out;
+  auto add = [&out](const char* s) { out += out.empty() ? s : std::string("; ") + s; };
+  if (st & (DBS_STATUS_LOOKBACK | DBS_STATUS_FIND | DBS_STATUS_BARRIER))
+    add("a bounded wait in the pipeline ran out");
+  if (st & DBS_STATUS_KEYSPACE) add("the clouds' cell-key ranges overflow 64 bits");
+  if (st & DBS_STATUS_CAPACITY) add("a work list exceeded its capacity (too many union-find cell pairs)");
+  if (out.empty()) add("unknown status bits");
+  return out;
+}
+
 void raise_if_failed(uint32_t st) {
   TORCH_CHECK(st == 0, "dbscan2d: device-side failure in an earlier call (status 0x",
-              std::hex, st, std::dec,
-              "): a bounded wait in the pipeline ran out; labels of that call are invalid");
+              std::hex, st, std::dec, "): ", status_text(st), "; labels of that call are invalid");
 }
 
 // Checks completed slots (all slots, waiting, when `wait`).
@@ -297,8 +308,8 @@ torch::Tensor run_host(const torch::Tensor& Xh, double eps, int64_t min_samples)
   if (rc == DBS_ERR_DEVICE) {
     uint32_t st = 0;
     check_rc(dbs_read_status(ws.data_ptr(), stream, &st), "dbscan2d");
-    TORCH_CHECK(false, "dbscan2d: device-side failure (status 0x", std::hex, st, std::dec,
-                "): a bounded wait in the pipeline ran out");
+    TORCH_CHECK(false, "dbscan2d: device-side failure (status 0x", std::hex, st, std::dec, "): ",
+                status_text(st));
   }
   check_rc(rc, "dbscan2d");
   return labels;
