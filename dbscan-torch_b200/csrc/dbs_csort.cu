@@ -7,9 +7,9 @@
 //
 // When the compacted key range is dense (every cloud within 6N + 4096 keys,
 // or all clouds of a batch within that budget summed -- the rule that gives
-// clouds a dense cell map), the sort needs no
-// radix passes: a key *is* its bin. Two ordinary launches, then one
-// cooperative kernel with phases separated by grid barriers:
+// clouds a dense cell map), the sort needs no radix passes: a key *is* its
+// bin. Two ordinary launches, then one cooperative kernel with phases
+// separated by grid barriers:
 //   0. clear the per-key counters (k_csort_clear)
 //   1. count points per key (k_csort_count; atomics aggregated over lanes
 //      with equal keys, so a 2M-point cell costs about one atomic per warp,

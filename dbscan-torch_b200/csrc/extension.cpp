@@ -159,7 +159,7 @@ torch::Tensor require_cuda_copy(const torch::Tensor& X) {
 }
 
 // ----------------------------------------------------------- graph replay
-// The plain call's launch sequence (21+ kernels, no host read-back) is
+// The plain call's launch sequence (23 kernels, no host read-back) is
 // replayed as a CUDA graph. Each device keeps a few executable graphs keyed
 // by the exact call (input, label and workspace pointers, n, eps,
 // min_samples): a repeated call -- the same buffers, or a loop alternating
