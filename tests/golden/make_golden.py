@@ -4,9 +4,9 @@ Runs ryanirl/dbscan-torch's CUDA path (built from its sources by
 oracle/build_ref.py into oracle/_ref/cuda) on small seeded inputs and stores,
 per case, the input, eps, min_samples, the labels and the per-stage
 intermediates of its debug entry point (dbscan_cuda.cu:777-789). Needs a GPU;
-run on the B200 box, then copy the .npz files next to this script:
+run it on a B200, then copy the .npz files from OUTDIR next to this script:
 
-    python tests/golden/make_golden.py --out gpurun_out/golden
+    python tests/golden/make_golden.py --out OUTDIR
 
 tests/test_oracle.py checks the CPU oracle against every fixture bit for bit.
 """
