@@ -62,19 +62,22 @@ __device__ __forceinline__ void rle_body(const Plan& p, K* s_keys, uint32_t* s_w
     }
     if (lane == 31) s_warp[warp] = x;
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (warp == 0) {  // the whole warp walks the look-back
       uint32_t run = 0;
-      for (int w = 0; w < nwarps; ++w) { const uint32_t t = s_warp[w]; s_warp[w] = run; run += t; }
+      if (lane == 0)
+        for (int w = 0; w < nwarps; ++w) { const uint32_t t = s_warp[w]; s_warp[w] = run; run += t; }
+      run = __shfl_sync(0xffffffffu, run, 0);
       unsigned long long* my = p.rle_status + tile;
       unsigned long long excl = 0;
-      if (tile == 0) st_relaxed(my, kFlagInc | run);
-      else {
-        st_relaxed(my, kFlagAgg | run);
-        excl = lookback(p.rle_status, tile, 1, d);
-        st_relaxed(my, kFlagInc | (excl + run));
+      if (tile == 0) {
+        if (lane == 0) st_relaxed(my, kFlagInc | run);
+      } else {
+        if (lane == 0) st_relaxed(my, kFlagAgg | run);
+        excl = lookback_warp(p.rle_status, tile, 1, d);
+        if (lane == 0) st_relaxed(my, kFlagInc | (excl + run));
       }
-      *s_excl = excl;
-      if (base + valid == n) {
+      if (lane == 0) *s_excl = excl;
+      if (lane == 0 && base + valid == n) {
         uint32_t total = (uint32_t)(excl + run);
         if ((int64_t)total > n) total = (uint32_t)n;  // only after a failed look-back
         d->num_cells = total;

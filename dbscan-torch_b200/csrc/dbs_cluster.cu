@@ -259,13 +259,15 @@ __global__ void __launch_bounds__(256) k_pairs(Plan p, int ring, int skip_united
         if (k >= nofs) continue;
         const int32_t nb = row[kRingOffs[ring][k]];
         if (nb <= (int32_t)c || p.cell_status[nb] == 0) continue;
-        if (!(box_box_d2(bb_c, p.bbox[nb]) <= eps_sq)) continue;
         if (skip_united) {
           // The flatten just before left every cell pointing at its root,
           // and no union runs during this kernel: one load is the find.
+          // Checked before the box (a 4-byte load against 16): in dense
+          // regions most pass-1 neighbours are joined already.
           if (root_c < 0) root_c = p.uf[c];
           if (p.uf[nb] == root_c) continue;
         }
+        if (!(box_box_d2(bb_c, p.bbox[nb]) <= eps_sq)) continue;
         mask |= 1u << k;
       }
     }
@@ -417,18 +419,21 @@ __global__ void __launch_bounds__(kScanThreads) k_ids(Plan p) {
     }
     if (lane == 31) s_warp[warp] = x;
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (warp == 0) {  // the whole warp walks the look-back
       uint32_t run = 0;
-      for (int wi = 0; wi < nwarps; ++wi) { const uint32_t t = s_warp[wi]; s_warp[wi] = run; run += t; }
+      if (lane == 0)
+        for (int wi = 0; wi < nwarps; ++wi) { const uint32_t t = s_warp[wi]; s_warp[wi] = run; run += t; }
+      run = __shfl_sync(kFull, run, 0);
       unsigned long long* my = p.ids_status + tile;
       unsigned long long excl = 0;
-      if (tile == 0) st_relaxed(my, kFlagInc | run);
-      else {
-        st_relaxed(my, kFlagAgg | run);
-        excl = lookback(p.ids_status, tile, 1, d);
-        st_relaxed(my, kFlagInc | (excl + run));
+      if (tile == 0) {
+        if (lane == 0) st_relaxed(my, kFlagInc | run);
+      } else {
+        if (lane == 0) st_relaxed(my, kFlagAgg | run);
+        excl = lookback_warp(p.ids_status, tile, 1, d);
+        if (lane == 0) st_relaxed(my, kFlagInc | (excl + run));
       }
-      s_excl = excl;
+      if (lane == 0) s_excl = excl;
     }
     __syncthreads();
     uint32_t rnk = (uint32_t)s_excl + s_warp[warp] + x - cnt;

@@ -287,32 +287,38 @@ constexpr unsigned long long kFlagInc = 2ull << 62;
 constexpr unsigned long long kValMask = (1ull << 62) - 1;
 
 // Decoupled look-back over look-back words laid out with `stride` between
-// consecutive tiles. Returns the exclusive prefix of tile `tile`. Each poll
-// reads a window of kLookWindow predecessors with independent loads, so a
-// walk over many published aggregates costs one round trip per window.
-// Bounded: a wait that exceeds kSpinCap polls sets kErrLookback and gives up.
-constexpr int kLookWindow = 8;
-
-__device__ __forceinline__ unsigned long long lookback(const unsigned long long* words,
-                                                       int64_t tile, int64_t stride, Desc* d) {
+// consecutive tiles, walked by a whole warp (all 32 lanes call it with the
+// same arguments); returns the exclusive prefix of tile `tile`. Each round
+// reads the 32 nearest unconsumed predecessors at once, consumes them up to
+// the first one not yet published and stops at the first inclusive prefix,
+// so a walk over many published aggregates costs one round trip per 32
+// tiles. Bounded: a wait that exceeds kSpinCap polls sets kErrLookback and
+// gives up.
+__device__ __forceinline__ unsigned long long lookback_warp(const unsigned long long* words,
+                                                            int64_t tile, int64_t stride, Desc* d) {
+  const uint32_t full = 0xffffffffu;
+  const int lane = (int)(threadIdx.x & 31u);
   unsigned long long excl = 0;
-  int64_t j = tile - 1;
+  int64_t j = tile - 1;  // nearest predecessor not consumed yet
   uint32_t spins = 0;
   while (j >= 0) {
-    unsigned long long v[kLookWindow];
+    const int64_t idx = j - lane;
+    // Before tile 0 there is nothing: an inclusive prefix of zero.
+    const unsigned long long v = idx >= 0 ? ld_relaxed(words + idx * stride) : kFlagInc;
+    const unsigned long long flag = v & ~kValMask;
+    const uint32_t not_ready = __ballot_sync(full, flag == 0);
+    const uint32_t inclusive = __ballot_sync(full, flag == kFlagInc);
+    const int first_nr = not_ready ? __ffs(not_ready) - 1 : 32;
+    const int first_inc = inclusive ? __ffs(inclusive) - 1 : 32;
+    const bool done = first_inc < first_nr;
+    const int take = done ? first_inc + 1 : first_nr;  // lanes [0, take) are consumed
+    unsigned long long part = lane < take ? (v & kValMask) : 0ull;
 #pragma unroll
-    for (int k = 0; k < kLookWindow; ++k)
-      v[k] = (j - k >= 0) ? ld_relaxed(words + (j - k) * stride) : kFlagInc;
-    int k = 0;
-#pragma unroll
-    for (; k < kLookWindow; ++k) {
-      const unsigned long long flag = v[k] & ~kValMask;
-      if (flag == 0) break;
-      excl += v[k] & kValMask;
-      if (flag == kFlagInc) return excl;
-    }
-    j -= k;
-    if (k < kLookWindow && ++spins > kSpinCap) {
+    for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(full, part, o);
+    excl += part;
+    if (done) return excl;
+    j -= take;
+    if (take < 32 && ++spins > kSpinCap) {
       set_error(d, kErrLookback);
       break;
     }
