@@ -39,6 +39,7 @@ size_t carve(int64_t n, int32_t nseg, char* base, Plan* p) {
   Carver cv{base};
   const size_t N = (size_t)(n > 0 ? n : 1);
   const int32_t scan_tiles = (int32_t)((N + kScanTile - 1) / kScanTile);
+  const int32_t ids_tiles = (int32_t)((N + kIdsTile - 1) / kIdsTile);
   q.desc = cv.take<Desc>(1);
   q.seg_off = cv.take<int64_t>((size_t)nseg + 1);
   q.seg_param = cv.take<SegParam>((size_t)nseg);
@@ -52,7 +53,7 @@ size_t carve(int64_t n, int32_t nseg, char* base, Plan* p) {
   q.is_core = cv.take<uint8_t>(N);
   q.chunk_count = cv.take<uint32_t>((size_t)kRadix * kMaxChunks);
   q.rle_status = cv.take<unsigned long long>((size_t)scan_tiles);
-  q.ids_status = cv.take<unsigned long long>((size_t)scan_tiles);
+  q.ids_status = cv.take<unsigned long long>((size_t)ids_tiles);
   q.point_cell = cv.take<int32_t>(N);
   q.cell_start = cv.take<int32_t>(N + 1);
   q.cell_key = cv.take<uint64_t>(N);
@@ -87,6 +88,7 @@ size_t carve(int64_t n, int32_t nseg, char* base, Plan* p) {
   q.n = n;
   q.nseg = nseg;
   q.scan_tiles = scan_tiles;
+  q.ids_tiles = ids_tiles;
   if (p) *p = q;
   return cv.off;
 }

@@ -363,61 +363,65 @@ __global__ void __launch_bounds__(256) k_flatten(Plan p) {
 // Flatten every cell to its root (read-only walk, dbscan_cuda.cu:374-378) and
 // rank the roots of non-noise components in cell order with a decoupled
 // look-back exclusive scan (dbscan_cuda.cu:383-404, 698-701).
+//
+// A tile is kIdsTile consecutive cells; warp w of the block owns the
+// 32 * kIdsItems cells from tile_base + w * 32 * kIdsItems, row k of them
+// (cells + k * 32 + lane) in item k of its lanes. Every load and store of the
+// uf, cell_status and root_rank arrays is then a whole-warp contiguous access,
+// and the rank of a root inside its warp is the popcount of the root-flag
+// ballots of the rows before it and of the lanes before it in its row.
 __global__ void __launch_bounds__(kScanThreads) k_ids(Plan p) {
   __shared__ uint32_t s_warp[kScanThreads / 32];
   __shared__ uint32_t s_tile;
   __shared__ unsigned long long s_excl;
   Desc* d = p.desc;
   const uint32_t C = d->num_cells;
-  const int64_t tiles = ((int64_t)C + kScanTile - 1) / kScanTile;
+  const int64_t tiles = ((int64_t)C + kIdsTile - 1) / kIdsTile;
   const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
+  const uint32_t lt = lanemask_lt();
   const int nwarps = blockDim.x >> 5;
   while (true) {
     if (threadIdx.x == 0) s_tile = atomicAdd(&d->ctr[kCtrIds], 1u);
     __syncthreads();
     const int64_t tile = s_tile;
     if (tile >= tiles) break;
-    const int64_t c0 = tile * kScanTile + (int64_t)threadIdx.x * kScanItems;
-    // Roots of the thread's cells, the walks advanced in lockstep: each round
+    const int64_t c0 = tile * kIdsTile + (int64_t)warp * 32 * kIdsItems + lane;
+    // Roots of the lane's cells, the walks advanced in lockstep: each round
     // issues one independent load per unfinished walk instead of finishing
     // one walk before starting the next.
-    int32_t r[kScanItems];
+    int32_t r[kIdsItems];
     uint32_t open = 0;
 #pragma unroll
-    for (int k = 0; k < kScanItems; ++k) {
-      const int64_t c = c0 + k;
+    for (int k = 0; k < kIdsItems; ++k) {
+      const int64_t c = c0 + k * 32;
       r[k] = c < C ? p.uf[c] : (int32_t)c;
       if (c < C && r[k] != (int32_t)c) open |= 1u << k;
     }
     for (uint32_t it = 0; open && it < kFindCap; ++it) {
-      int32_t nx[kScanItems];
+      int32_t nx[kIdsItems];
 #pragma unroll
-      for (int k = 0; k < kScanItems; ++k) nx[k] = (open >> k) & 1u ? p.uf[r[k]] : r[k];
+      for (int k = 0; k < kIdsItems; ++k) nx[k] = (open >> k) & 1u ? p.uf[r[k]] : r[k];
 #pragma unroll
-      for (int k = 0; k < kScanItems; ++k) {
+      for (int k = 0; k < kIdsItems; ++k) {
         if (nx[k] == r[k]) open &= ~(1u << k);
         r[k] = nx[k];
       }
     }
     if (open) set_error(d, kErrFind);
-    uint32_t flags = 0, cnt = 0;
+    uint32_t ball[kIdsItems];
+    uint32_t cnt = 0;
 #pragma unroll
-    for (int k = 0; k < kScanItems; ++k) {
-      const int64_t c = c0 + k;
+    for (int k = 0; k < kIdsItems; ++k) {
+      const int64_t c = c0 + k * 32;
+      bool f = false;
       if (c < C) {
         p.uf[c] = r[k];
-        const bool f = r[k] == (int32_t)c && p.cell_status[c] != 0;
-        flags |= (uint32_t)f << k;
-        cnt += f;
+        f = r[k] == (int32_t)c && p.cell_status[c] != 0;
       }
+      ball[k] = __ballot_sync(kFull, f);
+      cnt += __popc(ball[k]);
     }
-    uint32_t x = cnt;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t y = __shfl_up_sync(kFull, x, o);
-      if (lane >= (uint32_t)o) x += y;
-    }
-    if (lane == 31) s_warp[warp] = x;
+    if (lane == 0) s_warp[warp] = cnt;
     __syncthreads();
     if (warp == 0) {  // the whole warp walks the look-back
       uint32_t run = 0;
@@ -436,14 +440,12 @@ __global__ void __launch_bounds__(kScanThreads) k_ids(Plan p) {
       if (lane == 0) s_excl = excl;
     }
     __syncthreads();
-    uint32_t rnk = (uint32_t)s_excl + s_warp[warp] + x - cnt;
+    uint32_t rnk = (uint32_t)s_excl + s_warp[warp];
 #pragma unroll
-    for (int k = 0; k < kScanItems; ++k) {
-      const int64_t c = c0 + k;
-      if (c < C) {
-        p.root_rank[c] = (int32_t)rnk;
-        rnk += (flags >> k) & 1u;
-      }
+    for (int k = 0; k < kIdsItems; ++k) {
+      const int64_t c = c0 + k * 32;
+      if (c < C) p.root_rank[c] = (int32_t)(rnk + __popc(ball[k] & lt));
+      rnk += __popc(ball[k]);
     }
     __syncthreads();
   }

@@ -43,6 +43,8 @@ constexpr int kMaxGrid = 4096;   // blocks of a cooperative launch (bound)
 constexpr int kScanThreads = 256;
 constexpr int kScanItems = 16;
 constexpr int kScanTile = kScanThreads * kScanItems;
+constexpr int kIdsItems = 8;                    // cells per lane of a k_ids tile
+constexpr int kIdsTile = kScanThreads * kIdsItems;
 constexpr int kCellThreads = 256;               // warp-per-cell kernels
 constexpr uint32_t kSpinCap = 1u << 22;         // bounded waits (look-back polls)
 constexpr uint32_t kFindCap = 1u << 20;         // bounded union-find walks / retries
@@ -185,6 +187,7 @@ struct Plan {
   int32_t sort_chunks;    // chunks of the radix passes (one block each)
   int32_t chunk_tiles;    // kSortTile tiles per chunk
   int32_t scan_tiles;     // ceil(n / kScanTile)
+  int32_t ids_tiles;      // ceil(n / kIdsTile)
   int32_t num_sms;
   int32_t single;         // one cloud: k_init writes seg_off / seg_param
   SegParam single_param;

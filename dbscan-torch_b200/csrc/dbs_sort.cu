@@ -42,7 +42,8 @@ __global__ void k_init(Plan p) {
   }
   for (int64_t i = tid; i < 2 * kRadix; i += stride) (&d->digit_total[0][0])[i] = 0;
   if (tid == 0) { d->bar.count = 0; d->bar.gen = 0; d->dense_sort = 0; d->q_count = 0; d->b_count = 0; d->p_count = 0; d->d_count = 0; }
-  for (int64_t i = tid; i < p.scan_tiles; i += stride) { p.rle_status[i] = 0; p.ids_status[i] = 0; }
+  for (int64_t i = tid; i < p.scan_tiles; i += stride) p.rle_status[i] = 0;
+  for (int64_t i = tid; i < p.ids_tiles; i += stride) p.ids_status[i] = 0;
   if (p.single && tid == 0) {
     p.seg_off[0] = 0;
     p.seg_off[1] = p.n;
@@ -585,7 +586,7 @@ static int grid_for(const Plan& p, int64_t work, int threads, int per_sm) {
 }
 
 cudaError_t launch_front(const Plan& p, cudaStream_t s) {
-  k_init<<<grid_for(p, (int64_t)p.nseg + p.scan_tiles + 2 * kRadix, 256, 2), 256, 0, s>>>(p);
+  k_init<<<grid_for(p, (int64_t)p.nseg + p.ids_tiles + 2 * kRadix, 256, 2), 256, 0, s>>>(p);
   k_bounds<<<grid_for(p, p.n, 256 * 8, 8), 256, 0, s>>>(p);
   k_seg_finalize<<<1, 1024, 0, s>>>(p);
   return cudaGetLastError();
