@@ -444,8 +444,10 @@ def run_batched(dev, n_clouds: int) -> dict:
     """Config 3: n_clouds independent clouds (sizes log-uniform in [256, 262144],
     eps_i in [0.2, 1.0], min_samples_i in {4..32}) clustered by one batched
     pipeline run, against a loop of plain calls over the same device-resident
-    clouds. Both timed with CUDA events; labels compared cloud by cloud."""
-    from dbscan_torch import dbscan2d, dbscan2d_batched, synthetic
+    clouds. Both timed with CUDA events; labels compared cloud by cloud.
+    Then the same batch through a BatchedPlan (CUDA graph replay) with the
+    built-in launch shape and with the shape BatchedPlan.tune() picks."""
+    from dbscan_torch import BatchedPlan, dbscan2d, dbscan2d_batched, synthetic
     sizes, eps, ms = batch_config(n_clouds)
     X, off = synthetic.blobs_with_noise_device(sizes, seed=0, device=dev)
     offl = off.tolist()
@@ -462,9 +464,22 @@ def run_batched(dev, n_clouds: int) -> dict:
     tp, labs = _ev_ms(loop)
     equal = all(torch.equal(labs[k], lab_b[offl[k]:offl[k + 1]]) for k in range(n_clouds))
     _C_check()
+    del labs
+    torch.cuda.empty_cache()
+    plan = BatchedPlan(offl)
+    plan.run(X, eps, ms)  # captures the graph (built-in shape)
+    t_plan = statistics.median([_ev_ms(plan.run)[0] for _ in range(3)])
+    t0 = time.perf_counter()
+    tuned = plan.tune()
+    tune_s = time.perf_counter() - t0
+    plan.run()  # captures the graph with the tuned shape
+    t_tuned = statistics.median([_ev_ms(plan.run)[0] for _ in range(3)])
+    equal_tuned = torch.equal(plan.labels, lab_b)
+    if plan.status() != 0:
+        raise RuntimeError("batched plan: device status non-zero")
     t_b = statistics.median(tb)
     n_pts = int(offl[-1])
-    del X, lab_b, labs
+    del X, lab_b, plan
     torch.cuda.empty_cache()
     return {"workload": f"{n_clouds} clouds, N_i log-uniform [256, 262144], eps_i U[0.2, 1.0], "
                         f"min_samples_i U{{4..32}} (device generator, seed 0)",
@@ -472,7 +487,13 @@ def run_batched(dev, n_clouds: int) -> dict:
             "batched_ms": round(t_b, 3), "batched_clouds_per_s": round(n_clouds / (t_b * 1e-3), 1),
             "batched_mpoints_per_s": round(n_pts / (t_b * 1e-3) / 1e6, 1),
             "plain_loop_ms": round(tp, 3), "plain_loop_clouds_per_s": round(n_clouds / (tp * 1e-3), 1),
-            "speedup": round(tp / t_b, 2), "labels_equal": bool(equal)}
+            "speedup": round(tp / t_b, 2), "labels_equal": bool(equal),
+            "plan": {"graph_ms": round(t_plan, 3), "tuned_graph_ms": round(t_tuned, 3),
+                     "tuned_shape": dict(zip(("count", "cell_prep", "core", "pairs", "pair_scan", "labels"),
+                                             tuned["shape"])),
+                     "builtin_shape": list(tuned["default_shape"]),
+                     "tune_s": round(tune_s, 2), "shapes_timed": tuned["trials"],
+                     "labels_equal": bool(equal_tuned)}}
 
 
 def run_configs(dev) -> dict:

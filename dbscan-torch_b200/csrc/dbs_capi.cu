@@ -14,6 +14,12 @@
 #include "../../include/dbscan_b200.h"
 #include "dbs_internal.cuh"
 
+static_assert(dbs::kNumTuned == DBS_NUM_TUNED && dbs::kTuneCount == DBS_TUNE_COUNT &&
+                  dbs::kTuneCellPrep == DBS_TUNE_CELL_PREP && dbs::kTuneCore == DBS_TUNE_CORE &&
+                  dbs::kTunePairs == DBS_TUNE_PAIRS && dbs::kTunePairScan == DBS_TUNE_PAIR_SCAN &&
+                  dbs::kTuneLabels == DBS_TUNE_LABELS,
+              "launch-shape indices of the C-ABI and the pipeline differ");
+
 namespace dbs {
 namespace {
 
@@ -89,6 +95,7 @@ size_t carve(int64_t n, int32_t nseg, char* base, Plan* p) {
   q.nseg = nseg;
   q.scan_tiles = scan_tiles;
   q.ids_tiles = ids_tiles;
+  for (int k = 0; k < kNumTuned; ++k) q.bps[k] = kDefaultBlocksPerSm[k];
   if (p) *p = q;
   return cv.off;
 }
@@ -320,9 +327,27 @@ int dbs_fill_seg_params(const double* eps, const int64_t* min_samples, int32_t n
   return DBS_OK;
 }
 
+int dbs_default_launch_shape(dbs_launch_shape* out) {
+  if (out == nullptr) return DBS_ERR_INVALID;
+  for (int k = 0; k < kNumTuned; ++k) out->blocks_per_sm[k] = kDefaultBlocksPerSm[k];
+  return DBS_OK;
+}
+
 int dbs_dbscan2d_batched_device(const float* X, int64_t n_total, int32_t nseg,
                                 const int64_t* seg_offsets_dev, const void* seg_params_dev,
                                 int32_t* labels, void* ws, size_t ws_bytes, void* stream) {
+  return dbs_dbscan2d_batched_device_shaped(X, n_total, nseg, seg_offsets_dev, seg_params_dev, labels,
+                                            ws, ws_bytes, nullptr, stream);
+}
+
+int dbs_dbscan2d_batched_device_shaped(const float* X, int64_t n_total, int32_t nseg,
+                                       const int64_t* seg_offsets_dev, const void* seg_params_dev,
+                                       int32_t* labels, void* ws, size_t ws_bytes,
+                                       const dbs_launch_shape* shape, void* stream) {
+  if (shape != nullptr)
+    for (int k = 0; k < kNumTuned; ++k)
+      if (shape->blocks_per_sm[k] < 0 || shape->blocks_per_sm[k] > DBS_SHAPE_MAX_BLOCKS_PER_SM)
+        return DBS_ERR_INVALID;
   if (n_total < 0 || nseg < 1 || seg_offsets_dev == nullptr || seg_params_dev == nullptr)
     return DBS_ERR_INVALID;
   if (n_total > (int64_t)INT32_MAX) return DBS_ERR_TOO_LARGE;
@@ -342,6 +367,9 @@ int dbs_dbscan2d_batched_device(const float* X, int64_t n_total, int32_t nseg,
   p.X = reinterpret_cast<const float2*>(X);
   p.labels = labels;
   p.num_sms = num_sms_current();
+  if (shape != nullptr)
+    for (int k = 0; k < kNumTuned; ++k)
+      if (shape->blocks_per_sm[k] > 0) p.bps[k] = shape->blocks_per_sm[k];
   set_chunking(&p);
   p.single = 0;
   return run_pipeline(p, s, nullptr);

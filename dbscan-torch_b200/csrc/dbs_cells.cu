@@ -405,7 +405,7 @@ cudaError_t launch_rle(const Plan& p, cudaStream_t s) {
 }
 
 cudaError_t launch_cell_prep(const Plan& p, cudaStream_t s) {
-  k_cell_prep<<<p.num_sms * 8, kCellThreads, 0, s>>>(p);
+  k_cell_prep<<<p.num_sms * p.bps[kTuneCellPrep], kCellThreads, 0, s>>>(p);
   k_huge_bbox<<<p.num_sms * 4, 256, 0, s>>>(p);
   return cudaGetLastError();
 }

@@ -533,7 +533,7 @@ __global__ void __launch_bounds__(kCellThreads) k_labels(Plan p) {
 
 // ------------------------------------------------------------- launchers
 cudaError_t launch_core(const Plan& p, cudaStream_t s) {
-  k_core<<<p.num_sms * 8, kCellThreads, 0, s>>>(p);
+  k_core<<<p.num_sms * p.bps[kTuneCore], kCellThreads, 0, s>>>(p);
   k_status<<<p.num_sms * 8, 256, 0, s>>>(p);
   return cudaGetLastError();
 }
@@ -541,8 +541,8 @@ cudaError_t launch_core(const Plan& p, cudaStream_t s) {
 cudaError_t launch_union(const Plan& p, cudaStream_t s) {
   for (int ring = 0; ring < 2; ++ring) {
     if (ring == 1) k_flatten<<<p.num_sms * 8, 256, 0, s>>>(p);
-    k_pairs<<<p.num_sms * 8, 256, 0, s>>>(p, ring, ring);
-    k_pair_scan<<<p.num_sms * 8, 256, 0, s>>>(p);
+    k_pairs<<<p.num_sms * p.bps[kTunePairs], 256, 0, s>>>(p, ring, ring);
+    k_pair_scan<<<p.num_sms * p.bps[kTunePairScan], 256, 0, s>>>(p);
     k_pair_warp<<<p.num_sms * 8, 256, 0, s>>>(p);
   }
   return cudaGetLastError();
@@ -555,7 +555,7 @@ cudaError_t launch_ids(const Plan& p, cudaStream_t s) {
 
 cudaError_t launch_labels(const Plan& p, cudaStream_t s) {
   k_cid<<<p.num_sms * 4, 256, 0, s>>>(p);
-  k_labels<<<p.num_sms * 8, kCellThreads, 0, s>>>(p);
+  k_labels<<<p.num_sms * p.bps[kTuneLabels], kCellThreads, 0, s>>>(p);
   return cudaGetLastError();
 }
 

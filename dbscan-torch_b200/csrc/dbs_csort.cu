@@ -383,7 +383,7 @@ cudaError_t launch_csort(const Plan& p, cudaStream_t s) {
     if (blocks_per_sm < 1) return cudaErrorLaunchOutOfResources;
   }
   k_csort_clear<<<p.num_sms * 4, kCsThreads, 0, s>>>(p);
-  k_csort_count<<<p.num_sms * 8, kCsThreads, 0, s>>>(p);
+  k_csort_count<<<p.num_sms * p.bps[kTuneCount], kCsThreads, 0, s>>>(p);
   int grid = p.num_sms * blocks_per_sm;
   if (grid > kMaxGrid) grid = kMaxGrid;
   Plan q = p;

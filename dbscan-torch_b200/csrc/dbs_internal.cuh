@@ -60,6 +60,19 @@ constexpr int32_t kHugeChunk = 2048;  // points per chunk of a huge cell
 constexpr int64_t kDenseFactor = 6;
 constexpr int64_t kDenseSlack = 4096;
 
+// Grid-stride kernels whose grid (blocks per SM) a launch shape may set
+// (dbs_launch_shape of the C-ABI, same indices), and their built-in grids.
+enum : int {
+  kTuneCount = 0,
+  kTuneCellPrep,
+  kTuneCore,
+  kTunePairs,
+  kTunePairScan,
+  kTuneLabels,
+  kNumTuned
+};
+constexpr int32_t kDefaultBlocksPerSm[kNumTuned] = {8, 8, 8, 8, 8, 8};
+
 // Error bits of Desc::status (OR-ed by kernels, read by the host).
 enum : uint32_t {
   kErrLookback = 1u << 0,   // a decoupled look-back wait hit its cap
@@ -189,6 +202,7 @@ struct Plan {
   int32_t scan_tiles;     // ceil(n / kScanTile)
   int32_t ids_tiles;      // ceil(n / kIdsTile)
   int32_t num_sms;
+  int32_t bps[kNumTuned]; // blocks per SM of the tuned kernels
   int32_t single;         // one cloud: k_init writes seg_off / seg_param
   SegParam single_param;
 };

@@ -444,7 +444,7 @@ torch::Tensor dbscan2d_batched(torch::Tensor X, torch::Tensor seg_offsets, torch
 // CUDA tensor that stays alive across replays. params: uint8 (S*16) filled by
 // fill_seg_params; ws: uint8 of workspace_bytes(N, S).
 void dbscan2d_batched_into(torch::Tensor X, torch::Tensor seg_offsets_dev, torch::Tensor params_dev,
-                           torch::Tensor labels, torch::Tensor ws) {
+                           torch::Tensor labels, torch::Tensor ws, std::vector<int64_t> shape) {
   TORCH_CHECK(X.is_cuda() && seg_offsets_dev.is_cuda() && params_dev.is_cuda() && labels.is_cuda() &&
                   ws.is_cuda(),
               "all tensors must be on CUDA");
@@ -454,12 +454,27 @@ void dbscan2d_batched_into(torch::Tensor X, torch::Tensor seg_offsets_dev, torch
   TORCH_CHECK(labels.scalar_type() == torch::kInt32 && labels.numel() == X.size(0), "labels must be int32 (N,)");
   const int64_t S = seg_offsets_dev.numel() - 1;
   TORCH_CHECK(S >= 1 && params_dev.numel() == S * 16, "params must hold 16 bytes per cloud");
+  TORCH_CHECK(shape.empty() || shape.size() == DBS_NUM_TUNED, "shape must hold ", DBS_NUM_TUNED,
+              " entries (blocks per SM, 0 = built-in)");
+  dbs_launch_shape sh{};
+  for (size_t k = 0; k < shape.size(); ++k) {
+    TORCH_CHECK(shape[k] >= 0 && shape[k] <= DBS_SHAPE_MAX_BLOCKS_PER_SM, "shape entries must be in [0, ",
+                DBS_SHAPE_MAX_BLOCKS_PER_SM, "]");
+    sh.blocks_per_sm[k] = (int32_t)shape[k];
+  }
   c10::cuda::CUDAGuard guard(X.device());
   cudaStream_t stream = at::cuda::getCurrentCUDAStream();
-  check_rc(dbs_dbscan2d_batched_device(X.data_ptr<float>(), X.size(0), (int32_t)S,
-                                       seg_offsets_dev.data_ptr<int64_t>(), params_dev.data_ptr(),
-                                       labels.data_ptr<int32_t>(), ws.data_ptr(), ws.numel(), stream),
+  check_rc(dbs_dbscan2d_batched_device_shaped(X.data_ptr<float>(), X.size(0), (int32_t)S,
+                                              seg_offsets_dev.data_ptr<int64_t>(), params_dev.data_ptr(),
+                                              labels.data_ptr<int32_t>(), ws.data_ptr(), ws.numel(),
+                                              shape.empty() ? nullptr : &sh, stream),
            "dbscan2d_batched_into");
+}
+
+std::vector<int64_t> default_launch_shape() {
+  dbs_launch_shape sh{};
+  check_rc(dbs_default_launch_shape(&sh), "default_launch_shape");
+  return std::vector<int64_t>(sh.blocks_per_sm, sh.blocks_per_sm + DBS_NUM_TUNED);
 }
 
 torch::Tensor fill_seg_params(torch::Tensor eps, torch::Tensor min_samples) {
@@ -529,7 +544,11 @@ PYBIND11_MODULE(_C, m) {
         "Many clouds in one pipeline run; labels numbered per cloud.");
   m.def("dbscan2d_batched_into", &dbscan2d_batched_into, pybind11::arg("X"),
         pybind11::arg("seg_offsets"), pybind11::arg("params"), pybind11::arg("labels"),
-        pybind11::arg("ws"), "Batched run on device-resident buffers (CUDA-graph capturable).");
+        pybind11::arg("ws"), pybind11::arg("shape") = std::vector<int64_t>{},
+        "Batched run on device-resident buffers (CUDA-graph capturable); shape: blocks per SM of the "
+        "tuned kernels (empty = built-in).");
+  m.def("default_launch_shape", &default_launch_shape,
+        "Built-in blocks per SM of the tuned kernels (count, cell_prep, core, pairs, pair_scan, labels).");
   m.def("fill_seg_params", &fill_seg_params, pybind11::arg("eps"), pybind11::arg("min_samples"));
   m.def("workspace_bytes", &workspace_bytes, pybind11::arg("n"), pybind11::arg("nseg") = 1);
   m.def("read_status", &read_status, pybind11::arg("ws"));

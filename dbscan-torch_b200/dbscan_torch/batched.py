@@ -5,6 +5,8 @@ pipeline over all clouds. ``BatchedPlan`` keeps every buffer on the device
 for a fixed layout (cloud sizes) so that the whole pipeline -- about twenty
 kernel launches with no host synchronisation -- is captured once in a CUDA
 graph and replayed for each new batch of points / parameters.
+``BatchedPlan.tune()`` picks the grids of the pipeline's grid-stride kernels
+for the plan's layout (see ``tune.py``).
 """
 
 from __future__ import annotations
@@ -15,6 +17,7 @@ import numpy as np
 import torch
 
 from . import _C
+from . import tune as _tune
 
 
 class BatchedPlan:
@@ -46,6 +49,7 @@ class BatchedPlan:
         self._params_host = torch.zeros(self.nseg * 16, dtype=torch.uint8).pin_memory()
         self.use_graph = use_graph
         self.graph: Optional[torch.cuda.CUDAGraph] = None
+        self.shape: Optional[tuple] = None  # None = built-in launch shape
 
     def set_params(self, eps, min_samples) -> None:
         ep = torch.as_tensor(np.broadcast_to(np.asarray(eps, dtype=np.float64), (self.nseg,)).copy())
@@ -53,8 +57,55 @@ class BatchedPlan:
         self._params_host.copy_(_C.fill_seg_params(ep, ms))
         self.params.copy_(self._params_host, non_blocking=True)
 
-    def _launch(self) -> None:
-        _C.dbscan2d_batched_into(self.X, self.seg_offsets, self.params, self.labels, self.ws)
+    def _launch(self, shape=None) -> None:
+        shape = self.shape if shape is None else shape
+        _C.dbscan2d_batched_into(self.X, self.seg_offsets, self.params, self.labels, self.ws,
+                                 list(shape) if shape is not None else [])
+
+    def set_shape(self, shape) -> None:
+        """Launch shape for later runs: blocks per SM of the tuned kernels
+        (``tune.TUNED`` order; 0 = built-in), or None for the built-in shape.
+        A captured graph is dropped and captured again at the next run."""
+        if shape is not None:
+            shape = tuple(int(v) for v in shape)
+            if len(shape) != len(_tune.TUNED) or not all(0 <= v <= _tune.MAX_BLOCKS_PER_SM for v in shape):
+                raise ValueError(f"shape must hold {len(_tune.TUNED)} entries in [0, {_tune.MAX_BLOCKS_PER_SM}]")
+        self.shape = shape
+        self.graph = None
+
+    def tune(self, reps: int = 3, candidates: Sequence[int] = _tune.CANDIDATES, rounds: int = 1,
+             min_gain: float = 0.01) -> dict:
+        """Time launch shapes on the plan's current points and parameters
+        (eager launches on the current stream, CUDA events, best of ``reps``
+        runs per shape), keep the fastest for later runs and return
+        ``{"shape", "ms", "default_shape", "default_ms", "trials"}``. Labels
+        do not depend on the shape; the plan's labels afterwards are those of
+        the last shape timed."""
+        default = tuple(int(v) for v in _C.default_launch_shape())
+        if self.n == 0:
+            return {"shape": default, "ms": 0.0, "default_shape": default, "default_ms": 0.0, "trials": 0}
+        stream = torch.cuda.current_stream(self.device)
+
+        def measure(shape):
+            best = float("inf")
+            for _ in range(max(1, reps)):
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                self._launch(shape)
+                b.record(stream)
+                b.synchronize()
+                best = min(best, a.elapsed_time(b))
+            return best
+
+        start = self.shape if self.shape is not None and all(self.shape) else default
+        shape, t, trials = _tune.coordinate_descent(measure, start, candidates, rounds, min_gain)
+        st = self.status()
+        if st != 0:
+            raise RuntimeError(f"dbscan2d_batched: device status {st:#x} while tuning")
+        self.set_shape(shape)
+        return {"shape": shape, "ms": t, "default_shape": default, "default_ms": trials.get(default, float("nan")),
+                "trials": len(trials)}
 
     def run(self, X: Optional[torch.Tensor] = None, eps=None, min_samples=None) -> torch.Tensor:
         if X is not None:

@@ -111,6 +111,36 @@ int dbs_dbscan2d_batched_device(const float* X, int64_t n_total, int32_t nseg,
                                 const int64_t* seg_offsets_dev, const void* seg_params_dev,
                                 int32_t* labels, void* ws, size_t ws_bytes, void* stream);
 
+/* Launch shape (no counterpart in the reference, whose kernels take fixed
+ * grids sized by the work). blocks_per_sm[k] is the grid of tuned kernel k
+ * in blocks per SM; 0 keeps the built-in value (dbs_default_launch_shape).
+ * The tuned kernels all walk their work with grid-stride loops or dynamic
+ * work counters, so labels do not depend on the shape, only the time does.
+ * Valid entries: 0 .. DBS_SHAPE_MAX_BLOCKS_PER_SM. */
+#define DBS_NUM_TUNED 6
+#define DBS_TUNE_COUNT 0      /* per-key point counts of the counting sort */
+#define DBS_TUNE_CELL_PREP 1  /* cell boxes, neighbour rows, point classes */
+#define DBS_TUNE_CORE 2       /* core counts of the query points */
+#define DBS_TUNE_PAIRS 3      /* candidate cell pairs (both rings) */
+#define DBS_TUNE_PAIR_SCAN 4  /* pair tests and unions (both rings) */
+#define DBS_TUNE_LABELS 5     /* border assignment, core labels, unpermute */
+#define DBS_SHAPE_MAX_BLOCKS_PER_SM 32
+
+typedef struct dbs_launch_shape {
+  int32_t blocks_per_sm[DBS_NUM_TUNED];
+} dbs_launch_shape;
+
+/* The built-in shape (every entry non-zero). */
+int dbs_default_launch_shape(dbs_launch_shape* out);
+
+/* dbs_dbscan2d_batched_device with a launch shape (NULL = built-in). An entry
+ * outside 0 .. DBS_SHAPE_MAX_BLOCKS_PER_SM returns DBS_ERR_INVALID before any
+ * CUDA call. */
+int dbs_dbscan2d_batched_device_shaped(const float* X, int64_t n_total, int32_t nseg,
+                                       const int64_t* seg_offsets_dev, const void* seg_params_dev,
+                                       int32_t* labels, void* ws, size_t ws_bytes,
+                                       const dbs_launch_shape* shape, void* stream);
+
 /* Host helper: fills nseg 16-byte parameter records (see above). */
 int dbs_fill_seg_params(const double* eps, const int64_t* min_samples, int32_t nseg,
                         void* params_host);
