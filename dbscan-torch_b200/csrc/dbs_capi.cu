@@ -95,7 +95,7 @@ size_t carve(int64_t n, int32_t nseg, char* base, Plan* p) {
   q.nseg = nseg;
   q.scan_tiles = scan_tiles;
   q.ids_tiles = ids_tiles;
-  for (int k = 0; k < kNumTuned; ++k) q.bps[k] = kDefaultBlocksPerSm[k];
+  for (int k = 0; k < kNumTuned; ++k) q.bps[k] = default_blocks_per_sm(k, n);
   if (p) *p = q;
   return cv.off;
 }
@@ -327,9 +327,9 @@ int dbs_fill_seg_params(const double* eps, const int64_t* min_samples, int32_t n
   return DBS_OK;
 }
 
-int dbs_default_launch_shape(dbs_launch_shape* out) {
-  if (out == nullptr) return DBS_ERR_INVALID;
-  for (int k = 0; k < kNumTuned; ++k) out->blocks_per_sm[k] = kDefaultBlocksPerSm[k];
+int dbs_default_launch_shape(int64_t n_total, dbs_launch_shape* out) {
+  if (out == nullptr || n_total < 0) return DBS_ERR_INVALID;
+  for (int k = 0; k < kNumTuned; ++k) out->blocks_per_sm[k] = default_blocks_per_sm(k, n_total);
   return DBS_OK;
 }
 

@@ -479,7 +479,6 @@ __global__ void __launch_bounds__(256) k_cid(Plan p) {
 // input-order label writes of the clouds there -- together instead of
 // scattering them over the whole label array (3.5 ms against 7.6 ms for a
 // 151M-point, 4,096-cloud batch).
-constexpr int64_t kCoreFirstPoints = 16 << 20;
 
 __global__ void __launch_bounds__(kCellThreads) k_labels(Plan p) {
   const int64_t n = p.n;

@@ -62,6 +62,12 @@ constexpr int64_t kDenseSlack = 4096;
 
 // Grid-stride kernels whose grid (blocks per SM) a launch shape may set
 // (dbs_launch_shape of the C-ABI, same indices), and their built-in grids.
+// The label pass takes 32 blocks per SM while its border items go first
+// (n <= kCoreFirstPoints): they scan uneven numbers of neighbour points, and
+// smaller grid-stride shares balance them (10M constant-density points: 0.843
+// against 0.855 ms per call with 8). With the core items first (more points)
+// 8 blocks per SM is faster (4,096-cloud batch, 151M points: 22.1 against
+// 22.9 ms with 32).
 enum : int {
   kTuneCount = 0,
   kTuneCellPrep,
@@ -72,6 +78,15 @@ enum : int {
   kNumTuned
 };
 constexpr int32_t kDefaultBlocksPerSm[kNumTuned] = {8, 8, 8, 8, 8, 8};
+constexpr int32_t kLabelsBlocksPerSmBorderFirst = 32;
+// Label pass item order: border items first up to this many points (labels
+// that fit L2), core items first above (k_labels).
+constexpr int64_t kCoreFirstPoints = 16 << 20;
+// Built-in blocks per SM of tuned kernel k for a run over n points.
+inline int32_t default_blocks_per_sm(int k, int64_t n) {
+  if (k == kTuneLabels && n <= kCoreFirstPoints) return kLabelsBlocksPerSmBorderFirst;
+  return kDefaultBlocksPerSm[k];
+}
 
 // Error bits of Desc::status (OR-ed by kernels, read by the host).
 enum : uint32_t {

@@ -471,9 +471,9 @@ void dbscan2d_batched_into(torch::Tensor X, torch::Tensor seg_offsets_dev, torch
            "dbscan2d_batched_into");
 }
 
-std::vector<int64_t> default_launch_shape() {
+std::vector<int64_t> default_launch_shape(int64_t n) {
   dbs_launch_shape sh{};
-  check_rc(dbs_default_launch_shape(&sh), "default_launch_shape");
+  check_rc(dbs_default_launch_shape(n, &sh), "default_launch_shape");
   return std::vector<int64_t>(sh.blocks_per_sm, sh.blocks_per_sm + DBS_NUM_TUNED);
 }
 
@@ -547,8 +547,8 @@ PYBIND11_MODULE(_C, m) {
         pybind11::arg("ws"), pybind11::arg("shape") = std::vector<int64_t>{},
         "Batched run on device-resident buffers (CUDA-graph capturable); shape: blocks per SM of the "
         "tuned kernels (empty = built-in).");
-  m.def("default_launch_shape", &default_launch_shape,
-        "Built-in blocks per SM of the tuned kernels (count, cell_prep, core, pairs, pair_scan, labels).");
+  m.def("default_launch_shape", &default_launch_shape, pybind11::arg("n"),
+        "Built-in blocks per SM, for a run over n points, of the tuned kernels (count, cell_prep, core, pairs, pair_scan, labels).");
   m.def("fill_seg_params", &fill_seg_params, pybind11::arg("eps"), pybind11::arg("min_samples"));
   m.def("workspace_bytes", &workspace_bytes, pybind11::arg("n"), pybind11::arg("nseg") = 1);
   m.def("read_status", &read_status, pybind11::arg("ws"));

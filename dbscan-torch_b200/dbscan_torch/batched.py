@@ -81,7 +81,7 @@ class BatchedPlan:
         ``{"shape", "ms", "default_shape", "default_ms", "trials"}``. Labels
         do not depend on the shape; the plan's labels afterwards are those of
         the last shape timed."""
-        default = tuple(int(v) for v in _C.default_launch_shape())
+        default = tuple(int(v) for v in _C.default_launch_shape(self.n))
         if self.n == 0:
             return {"shape": default, "ms": 0.0, "default_shape": default, "default_ms": 0.0, "trials": 0}
         stream = torch.cuda.current_stream(self.device)

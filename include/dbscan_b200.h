@@ -130,8 +130,9 @@ typedef struct dbs_launch_shape {
   int32_t blocks_per_sm[DBS_NUM_TUNED];
 } dbs_launch_shape;
 
-/* The built-in shape (every entry non-zero). */
-int dbs_default_launch_shape(dbs_launch_shape* out);
+/* The built-in shape of a run over n_total points (every entry non-zero):
+ * 8 blocks per SM; the label pass 32 up to 2^24 points, 8 above. */
+int dbs_default_launch_shape(int64_t n_total, dbs_launch_shape* out);
 
 /* dbs_dbscan2d_batched_device with a launch shape (NULL = built-in). An entry
  * outside 0 .. DBS_SHAPE_MAX_BLOCKS_PER_SM returns DBS_ERR_INVALID before any

@@ -59,9 +59,13 @@ def test_capi_shape_checks():
     """Host-side checks only: no CUDA call is reached."""
     lib = ctypes.CDLL(LIB)
     sh = _Shape()
-    assert lib.dbs_default_launch_shape(ctypes.byref(sh)) == 0
+    lib.dbs_default_launch_shape.argtypes = [ctypes.c_int64, ctypes.c_void_p]
+    assert lib.dbs_default_launch_shape(10_000_000, ctypes.byref(sh)) == 0
+    assert list(sh.blocks_per_sm) == [8, 8, 8, 8, 8, 32]
+    assert lib.dbs_default_launch_shape((16 << 20) + 1, ctypes.byref(sh)) == 0
     assert list(sh.blocks_per_sm) == [8] * 6
-    assert lib.dbs_default_launch_shape(None) == 1
+    assert lib.dbs_default_launch_shape(10, None) == 1
+    assert lib.dbs_default_launch_shape(-1, ctypes.byref(sh)) == 1
     f = lib.dbs_dbscan2d_batched_device_shaped
     f.restype = ctypes.c_int
     f.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
@@ -117,15 +121,17 @@ def test_labels_do_not_depend_on_shape():
 
 @pytest.mark.gpu
 def test_tuned_plan_replays_same_labels():
-    from dbscan_torch import BatchedPlan, dbscan2d_batched
+    from dbscan_torch import BatchedPlan, _C, dbscan2d_batched
     clouds, X, off, eps, ms = _batch()
     Xd = torch.from_numpy(X).cuda()
     want = dbscan2d_batched(Xd, off.tolist(), eps.tolist(), ms.tolist()).cpu().numpy()
     plan = BatchedPlan(off.tolist())
     plan.run(Xd, eps, ms)
     res = plan.tune(reps=2, candidates=(4, 8, 16))
-    assert len(res["shape"]) == 6 and all(v in (4, 8, 16) for v in res["shape"])
-    assert res["default_shape"] == (8,) * 6 and res["ms"] <= res["default_ms"]
+    default = tuple(_C.default_launch_shape(int(off[-1])))
+    assert res["default_shape"] == default and res["ms"] <= res["default_ms"]
+    # Each entry is a candidate or the built-in value it started from.
+    assert len(res["shape"]) == 6 and all(v in (4, 8, 16) or v == d for v, d in zip(res["shape"], default))
     assert plan.shape == res["shape"]
     for _ in range(2):  # capture with the tuned shape, then replay
         assert np.array_equal(plan.run(Xd).cpu().numpy(), want)
