@@ -82,6 +82,21 @@ def test_capi_shape_checks():
     assert f(None, 0, 1, fake, fake, None, fake, 1 << 40, None, None) == 0
 
 
+def test_plan_set_shape_checks():
+    """BatchedPlan.set_shape validates on the host and drops a captured graph
+    (no device buffers needed: the plan object is built without __init__)."""
+    from dbscan_torch import BatchedPlan
+    plan = object.__new__(BatchedPlan)
+    plan.graph = object()
+    plan.set_shape([2, 4, 8, 16, 32, 0])
+    assert plan.shape == (2, 4, 8, 16, 32, 0) and plan.graph is None
+    for bad in [(8,) * 5, (8,) * 7, (33,) + (8,) * 5, (-1,) + (8,) * 5]:
+        with pytest.raises(ValueError):
+            plan.set_shape(bad)
+    plan.set_shape(None)
+    assert plan.shape is None
+
+
 def _batch():
     from dbscan_torch import synthetic
     rng = np.random.default_rng(21)
