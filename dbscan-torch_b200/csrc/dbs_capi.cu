@@ -91,6 +91,10 @@ size_t carve(int64_t n, int32_t nseg, char* base, Plan* p) {
   q.bin_count = cv.take<uint32_t>((size_t)q.dense_cap);
   q.blk_sum = cv.take<uint32_t>((size_t)kMaxGrid);
   q.blk_ne = cv.take<uint32_t>((size_t)kMaxGrid);
+  q.hot_key = cv.take<uint32_t>((size_t)kHotSlots);
+  q.hot_cnt = cv.take<uint32_t>((size_t)kHotSlots);
+  q.hot_cold = cv.take<uint32_t>((size_t)kHotSlots);
+  q.hot_base = cv.take<uint32_t>((size_t)kHotSlots);
   q.n = n;
   q.nseg = nseg;
   q.scan_tiles = scan_tiles;

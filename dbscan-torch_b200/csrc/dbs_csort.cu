@@ -96,6 +96,36 @@ __device__ __forceinline__ Agg aggregate(uint32_t key, bool valid) {
   return a;
 }
 
+// Hot-key table: open addressing with linear probing, insert-only, keyed by
+// the dense key (< 2^31, so never kHotEmpty). The count kernel inserts (a
+// key lands in the first slot of its probe sequence that is empty or holds
+// it, so every inserter and every later reader agrees on the slot); later
+// kernels only look keys up. A full table leaves further keys cold.
+constexpr uint32_t kHotEmpty = 0xffffffffu;
+
+__device__ __forceinline__ uint32_t hot_hash(uint32_t key) {
+  return (key * 2654435761u) >> 26;  // multiplicative hash, top 6 bits
+}
+
+__device__ __forceinline__ int hot_insert(const Plan& p, uint32_t key) {
+  uint32_t s = hot_hash(key);
+  for (int probe = 0; probe < kHotSlots; ++probe, s = (s + 1) & (kHotSlots - 1)) {
+    const uint32_t old = atomicCAS(&p.hot_key[s], kHotEmpty, key);
+    if (old == kHotEmpty || old == key) return (int)s;
+  }
+  return -1;
+}
+
+__device__ __forceinline__ int hot_find(const Plan& p, uint32_t key) {
+  uint32_t s = hot_hash(key);
+  for (int probe = 0; probe < kHotSlots; ++probe, s = (s + 1) & (kHotSlots - 1)) {
+    const uint32_t k = p.hot_key[s];
+    if (k == key) return (int)s;
+    if (k == kHotEmpty) return -1;
+  }
+  return -1;
+}
+
 // Cloud owning global key b: the last cloud whose key base is <= b (empty
 // clouds share their base with the next cloud and come before it).
 __device__ __forceinline__ int32_t seg_of_key(const Plan& p, uint64_t b) {
@@ -149,6 +179,18 @@ __device__ __forceinline__ void scan_bins(const Plan& p, int64_t W, uint32_t* s_
   // on 256-byte boundaries).
   const int64_t per = (((W + gridDim.x - 1) / gridDim.x) + kI - 1) & ~(int64_t)(kI - 1);
   const int64_t r0 = min(W, (int64_t)blockIdx.x * per), r1 = min(W, r0 + per);
+  // Hot keys in this block's range: their count so far covers only the points
+  // outside hot rows; add the hot rows' points (the block owns these keys, so
+  // no other block reads or writes them here).
+  if (threadIdx.x < kHotSlots) {
+    const uint32_t key = p.hot_key[threadIdx.x];
+    if (key != kHotEmpty && (int64_t)key >= r0 && (int64_t)key < r1) {
+      const uint32_t cold = bins[key];
+      p.hot_cold[threadIdx.x] = cold;
+      bins[key] = cold + p.hot_cnt[threadIdx.x];
+    }
+  }
+  __syncthreads();
   {
     uint32_t cs = 0, ne = 0;
     for (int64_t b = r0 + threadIdx.x; b < r1; b += blockDim.x) {
@@ -248,6 +290,14 @@ __device__ __forceinline__ void scan_bins(const Plan& p, int64_t W, uint32_t* s_
       carry_ne += tb;
     }
   }
+  // Hot points take the last slots of their key: after the cold points, which
+  // the scatter places by fetch-add from the key's first slot.
+  __syncthreads();
+  if (threadIdx.x < kHotSlots) {
+    const uint32_t key = p.hot_key[threadIdx.x];
+    if (key != kHotEmpty && (int64_t)key >= r0 && (int64_t)key < r1)
+      p.hot_base[threadIdx.x] = bins[key] + p.hot_cold[threadIdx.x];
+  }
   grid_sync(&d->bar, d);
 }
 
@@ -261,6 +311,7 @@ __global__ void __launch_bounds__(kCsThreads) k_csort_clear(Plan p) {
   const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t nthr = (int64_t)gridDim.x * blockDim.x;
   for (int64_t b = tid; b < W; b += nthr) p.bin_count[b] = 0;
+  if (tid < kHotSlots) { p.hot_key[tid] = kHotEmpty; p.hot_cnt[tid] = 0; }
 }
 
 __global__ void __launch_bounds__(kCsThreads, 6) k_csort_count(Plan p) {
@@ -268,7 +319,9 @@ __global__ void __launch_bounds__(kCsThreads, 6) k_csort_count(Plan p) {
   if (d->dense_sort != 1) return;
   const int64_t n = p.n;
   uint32_t* bins = p.bin_count;
+  uint32_t* rank = p.vals[0];  // hot points' ranks (the radix buffer is free here)
   const uint32_t lane = lane_id();
+  const uint32_t lt = lanemask_lt();
   const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t nthr = (int64_t)gridDim.x * blockDim.x;
   // Each warp takes kU consecutive 32-point rows per iteration;
@@ -294,7 +347,21 @@ __global__ void __launch_bounds__(kCsThreads, 6) k_csort_count(Plan p) {
           key = kc.key(v[k]);
         }
         const Agg a = aggregate(key, valid);
-        if (valid && lane == a.leader) atomicAdd(&bins[key], (uint32_t)__popc(a.group));
+        const uint32_t g = (uint32_t)__popc(a.group);
+        int slot = -1;
+        uint32_t pos = 0;
+        if (valid && lane == a.leader) {
+          if (g >= kHotGroup) slot = hot_insert(p, key);
+          if (slot >= 0) pos = atomicAdd(&p.hot_cnt[slot], g);
+          else atomicAdd(&bins[key], g);
+        }
+        // Rows are the aligned 32-point groups [32m, 32m + 32) whatever the
+        // grid, so the scatter sees the same groups and the same hot verdicts.
+        if (__any_sync(kFullMask, slot >= 0)) {
+          const int ls = __shfl_sync(kFullMask, slot, a.leader);
+          const uint32_t b0 = __shfl_sync(kFullMask, pos, a.leader);
+          if (valid && ls >= 0) rank[i] = b0 + __popc(a.group & lt);
+        }
       }
     }
   }
@@ -330,6 +397,7 @@ __global__ void __launch_bounds__(kCsThreads, 5) k_csort(Plan p) {
         v[k] = i < n ? p.X[i] : make_float2(0.f, 0.f);
       }
       uint32_t pos[kU];
+      int hot[kU];
       Agg ag[kU];
 #pragma unroll
       for (int k = 0; k < kU; ++k) {
@@ -341,13 +409,28 @@ __global__ void __launch_bounds__(kCsThreads, 5) k_csort(Plan p) {
         }
         ag[k] = aggregate(key, i < n);
         pos[k] = 0;
-        if (i < n && lane == ag[k].leader) pos[k] = atomicAdd(&bins[key], (uint32_t)__popc(ag[k].group));
+        hot[k] = 0;
+        if (i < n && lane == ag[k].leader) {
+          const uint32_t g = (uint32_t)__popc(ag[k].group);
+          const int slot = g >= kHotGroup ? hot_find(p, key) : -1;
+          if (slot >= 0) {
+            pos[k] = p.hot_base[slot];
+            hot[k] = 1;
+          } else {
+            pos[k] = atomicAdd(&bins[key], g);
+          }
+        }
       }
 #pragma unroll
       for (int k = 0; k < kU; ++k) {
         const int64_t i = base + k * 32 + lane;
-        const uint32_t at = __shfl_sync(kFullMask, pos[k], ag[k].leader) + __popc(ag[k].group & lt);
-        if (i < n) p.perm[at] = (uint32_t)i;
+        const int h = __shfl_sync(kFullMask, hot[k], ag[k].leader);
+        uint32_t at = __shfl_sync(kFullMask, pos[k], ag[k].leader);
+        if (i < n) {
+          at += h ? p.vals[0][i] : (uint32_t)__popc(ag[k].group & lt);
+          if ((int64_t)at < n) p.perm[at] = (uint32_t)i;
+          else set_error(d, kErrCapacity);
+        }
       }
     }
   }

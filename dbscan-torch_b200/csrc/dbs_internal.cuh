@@ -58,6 +58,11 @@ constexpr int32_t kHugeChunk = 2048;  // points per chunk of a huge cell
 // batch whose clouds' ranges fit the summed budget gets a map for every
 // cloud (k_seg_finalize).
 constexpr int64_t kDenseFactor = 6;
+// Counting sort: a key that at least kHotGroup lanes of one 32-point row
+// share is hot; up to kHotSlots hot keys get their points ranked by the count
+// pass instead of a second fetch-add in the scatter.
+constexpr int kHotSlots = 64;
+constexpr uint32_t kHotGroup = 8;
 constexpr int64_t kDenseSlack = 4096;
 
 // Grid-stride kernels whose grid (blocks per SM) a launch shape may set
@@ -209,6 +214,10 @@ struct Plan {
   uint32_t* bin_count;    // counting sort: per-key counts -> offsets -> cursors
   uint32_t* blk_sum;      // counting sort: per-block bin sums (kMaxGrid)
   uint32_t* blk_ne;       // counting sort: per-block non-empty bin counts
+  uint32_t* hot_key;      // counting sort: hot-key table (kHotSlots each)
+  uint32_t* hot_cnt;      //   points of hot rows per hot key
+  uint32_t* hot_cold;     //   points of the key outside hot rows
+  uint32_t* hot_base;     //   first sorted position of the key's hot points
   int32_t force_radix;    // debug entry: stable radix sort (reference perm)
   int64_t n;
   int32_t nseg;
