@@ -23,7 +23,10 @@
 //      the cells get cell_start / cell_key / cell_seg (the run-length cells of
 //      the reference, in the same ascending key order, without a pass over
 //      sorted keys)
-//   5. scatter every point's index to its key's next slot (perm)
+//   5. scatter every point's index to its key's next slot (perm); points of
+//      hot keys (shared by >= kHotGroup lanes of one 32-point row) were
+//      ranked by the count instead and go to the key's last slots without a
+//      second fetch-add on the key
 //   6. gather the sorted float2 coordinates point-parallel (coalesced writes)
 // Points inside one cell land in arrival order rather than input order. No
 // label depends on that order (core counts, cell-pair edges, boxes and the
@@ -384,7 +387,8 @@ __global__ void __launch_bounds__(kCsThreads, 5) k_csort(Plan p) {
   mark_phase(d, 3);
 
   // 5. scatter every point's input index to the slot its key's fetch-add
-  //    returns (perm)
+  //    returns (perm), or, in a hot row of a key in the hot table, to the
+  //    key's hot base plus the rank the count kernel gave it
   {
     const uint32_t lt = lanemask_lt();
     KeyCtx kc;
