@@ -99,12 +99,17 @@ __device__ __forceinline__ Agg aggregate(uint32_t key, bool valid) {
   return a;
 }
 
-// Hot-key table: open addressing with linear probing, insert-only, keyed by
-// the dense key (< 2^31, so never kHotEmpty). The count kernel inserts (a
-// key lands in the first slot of its probe sequence that is empty or holds
-// it, so every inserter and every later reader agrees on the slot); later
-// kernels only look keys up. A full table leaves further keys cold.
+// Hot-key table: open addressing with linear probing over a window of
+// kHotProbes slots, insert-only, keyed by the dense key (< 2^31, so never
+// kHotEmpty). The count kernel inserts: a key lands in the first slot of its
+// window that is empty or holds it, so every inserter and every later reader
+// agrees on the slot; later kernels only look keys up. A key whose window is
+// full stays cold (correct, only slower). Probes read first and
+// compare-and-swap only an empty slot, so once the table has filled (inputs
+// in spatial order make most rows hot) a row costs a few L2 reads, not a
+// queue of atomics on the table.
 constexpr uint32_t kHotEmpty = 0xffffffffu;
+constexpr int kHotProbes = 8;
 
 __device__ __forceinline__ uint32_t hot_hash(uint32_t key) {
   return (key * 2654435761u) >> 26;  // multiplicative hash, top 6 bits
@@ -112,16 +117,17 @@ __device__ __forceinline__ uint32_t hot_hash(uint32_t key) {
 
 __device__ __forceinline__ int hot_insert(const Plan& p, uint32_t key) {
   uint32_t s = hot_hash(key);
-  for (int probe = 0; probe < kHotSlots; ++probe, s = (s + 1) & (kHotSlots - 1)) {
-    const uint32_t old = atomicCAS(&p.hot_key[s], kHotEmpty, key);
-    if (old == kHotEmpty || old == key) return (int)s;
+  for (int probe = 0; probe < kHotProbes; ++probe, s = (s + 1) & (kHotSlots - 1)) {
+    uint32_t k = __ldcg(&p.hot_key[s]);
+    if (k == kHotEmpty) k = atomicCAS(&p.hot_key[s], kHotEmpty, key);  // the slot's old value
+    if (k == kHotEmpty || k == key) return (int)s;
   }
   return -1;
 }
 
 __device__ __forceinline__ int hot_find(const Plan& p, uint32_t key) {
   uint32_t s = hot_hash(key);
-  for (int probe = 0; probe < kHotSlots; ++probe, s = (s + 1) & (kHotSlots - 1)) {
+  for (int probe = 0; probe < kHotProbes; ++probe, s = (s + 1) & (kHotSlots - 1)) {
     const uint32_t k = p.hot_key[s];
     if (k == key) return (int)s;
     if (k == kHotEmpty) return -1;
@@ -322,9 +328,7 @@ __global__ void __launch_bounds__(kCsThreads, 6) k_csort_count(Plan p) {
   if (d->dense_sort != 1) return;
   const int64_t n = p.n;
   uint32_t* bins = p.bin_count;
-  uint32_t* rank = p.vals[0];  // hot points' ranks (the radix buffer is free here)
   const uint32_t lane = lane_id();
-  const uint32_t lt = lanemask_lt();
   const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t nthr = (int64_t)gridDim.x * blockDim.x;
   // Each warp takes kU consecutive 32-point rows per iteration;
@@ -363,7 +367,7 @@ __global__ void __launch_bounds__(kCsThreads, 6) k_csort_count(Plan p) {
         if (__any_sync(kFullMask, slot >= 0)) {
           const int ls = __shfl_sync(kFullMask, slot, a.leader);
           const uint32_t b0 = __shfl_sync(kFullMask, pos, a.leader);
-          if (valid && ls >= 0) rank[i] = b0 + __popc(a.group & lt);
+          if (valid && ls >= 0) p.vals[0][i] = b0 + __popc(a.group & lanemask_lt());
         }
       }
     }
