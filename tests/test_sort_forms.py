@@ -132,3 +132,28 @@ def test_batched_above_core_first_threshold():
     for k in range(len(sizes)):
         want = dbscan2d(X[offl[k]:offl[k + 1]], eps[k], ms[k])
         assert torch.equal(lab[offl[k]:offl[k + 1]], want), f"cloud {k}"
+
+
+@pytest.mark.parametrize("order", ["cell_order", "dominant_cell"])
+def test_hot_keys(order):
+    """Rows of 32 consecutive points that share a cell (hot keys) are ranked by
+    the count pass through a 64-slot table. Points in cell order make nearly
+    every row hot, so the table fills and later keys stay cold; a cloud with
+    most points in one cell keeps one key hot. Labels equal the oracle's."""
+    if order == "cell_order":
+        X = synthetic.constant_density(300_000, seed=8)
+        inv_r = np.float32(np.sqrt(np.float32(2.0)) / np.float32(EPS))
+        kx = np.floor(X[:, 0] * inv_r).astype(np.int64)
+        ky = np.floor(X[:, 1] * inv_r).astype(np.int64)
+        X = X[np.lexsort((ky, kx))]
+        ms = 10
+    else:
+        rng = np.random.default_rng(9)
+        X = synthetic.blobs_with_noise(200_000, seed=9, n_blobs=5)
+        X[:120_000] = rng.uniform(0.01, 0.05, size=(120_000, 2)).astype(np.float32)
+        X = X[rng.permutation(X.shape[0])]
+        ms = 4
+    ours, info = _C.dbscan2d_info(torch.from_numpy(X).cuda(), EPS, ms)
+    assert info["passes"] == 0, info  # the counting sort ran
+    want = oracle.dbscan2d(X, EPS, ms)
+    assert np.array_equal(ours.cpu().numpy(), want)
