@@ -99,7 +99,7 @@ enum : uint32_t {
   kErrFind = 1u << 1,       // a union-find walk / hook loop hit its cap
   kErrKeySpace = 1u << 2,   // batched key ranges overflow 64 bits
   kErrBarrier = 1u << 3,    // a grid barrier wait hit its cap
-  kErrCapacity = 1u << 4,   // a work list received more entries than it holds
+  kErrCapacity = 1u << 4,   // a work list overflowed, or a sorted position out of range
 };
 
 // Dynamic work counters (Desc::ctr).

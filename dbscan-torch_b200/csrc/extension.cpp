@@ -66,7 +66,7 @@ std::string status_text(uint32_t st) {
   if (st & (DBS_STATUS_LOOKBACK | DBS_STATUS_FIND | DBS_STATUS_BARRIER))
     add("a bounded wait in the pipeline ran out");
   if (st & DBS_STATUS_KEYSPACE) add("the clouds' cell-key ranges overflow 64 bits");
-  if (st & DBS_STATUS_CAPACITY) add("a work list exceeded its capacity (too many union-find cell pairs)");
+  if (st & DBS_STATUS_CAPACITY) add("a work list exceeded its capacity (too many union-find cell pairs) or a sorted position fell out of range");
   if (out.empty()) add("unknown status bits");
   return out;
 }

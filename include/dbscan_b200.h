@@ -50,7 +50,8 @@ extern "C" {
 #define DBS_STATUS_KEYSPACE 4u  /* batched cell-key ranges overflowed 64 bits */
 #define DBS_STATUS_BARRIER 8u   /* a grid-wide barrier wait reached its cap */
 #define DBS_STATUS_CAPACITY 16u /* a work list (union-find cell pairs, at most 2^32 - 1)
-                                   received more entries than it holds */
+                                   received more entries than it holds, or a sorted
+                                   position fell outside [0, n) (internal check) */
 
 #define DBS_NUM_STAGES 10
 
