@@ -14,37 +14,47 @@ synthetic data. One step = one dbscan2d call over the whole cloud.
   roofline  dominant stage: algorithmic bytes per launch / its average launch
             time (per-stage CUDA events of dbscan2d_profile), against the
             measured HBM copy bandwidth in MEASURED_PEAKS.json
-  cpu_baseline  the reference's own CPU implementation (built from its
+  cpu_baseline    the reference's own CPU implementation (built from its
             sources into oracle/_ref/cpu) on the box's host cores, timed on
-            the same workload
+            the same workload in a fresh child process before this process
+            touches the GPU
+  reference_cuda  the reference's own CUDA implementation (oracle/_ref/cuda)
+            on the same GPU and workload, in a child process run before this
+            process touches the GPU: same warm-up, L2 flush and CUDA events,
+            its per-stage split (dbscan2d_profile), and whether its labels
+            equal this build's
   configs   the other plain-call workloads on the device: 100k blobs with
             noise, constant density at 1M and 5M, the adversarial 4M cloud
             (min_samples 4 and 32) (--no-configs skips them)
   batched   4,096 clouds (sizes log-uniform in [256, 262144]) in one batched
             pipeline run vs a loop of plain calls: clouds/s of each
             (--batched-clouds; 0 skips)
-  serving   a Poisson request stream (2,000 req/s, sizes log-uniform in
-            [1e3, 2e6]) through the continuous-batching server vs sequential
-            plain calls: p50/p99 latency and clouds/s (--serve-seconds,
-            default 10 s of arrivals; 0 skips)
+  serving   the Poisson request stream (2,000 req/s, sizes log-uniform in
+            [1e3, 2e6], 60 s by default) through the continuous-batching
+            server and through sequential plain calls: p50/p99 latency and
+            clouds/s; then, for both, the highest offered rate whose p99 stays
+            within 50 ms (--serve-seconds; 0 skips)
 
---impl reference times only that reference CPU path and prints its line.
-Multi-GPU (torchrun): replicas only -- every rank clusters its own cloud;
-the time is the max over ranks.
+--impl reference times only the reference CPU path and prints its line (it
+imports nothing of this build). Multi-GPU (torchrun): replicas only -- every
+rank clusters its own cloud; the time is the max over ranks.
 """
 
 from __future__ import annotations
 
 import argparse
+import importlib.util
 import json
 import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
-sys.path.insert(0, os.path.join(ROOT, "dbscan-torch_b200"))
+PKG_DIR = os.path.join(ROOT, "dbscan-torch_b200")
+ORACLE_DIR = os.path.join(ROOT, "oracle")
 
 import numpy as np  # noqa: E402
 import torch  # noqa: E402
@@ -54,6 +64,7 @@ UNIT = "Mpoints/s"
 N_POINTS = 10_000_000
 EPS, MIN_SAMPLES = 0.5, 10
 WORKLOAD = "constant_density_10M"
+DATA = "synthetic (seeded constant-density Gaussian blobs + 2% noise)"
 L2_FLUSH_BYTES = 512 << 20
 # Kernel launches of one dbscan2d call (tests/test_launch_count.py counts them
 # with the profiler): init, bounds, seg_finalize | csort_clear, csort_count,
@@ -68,8 +79,39 @@ STAGE_LAUNCHES = {"cell_keys": 3, "sort_gather": 5, "boundary_scan": 1, "build_n
 # The kernels that do a stage's work on this workload (the others of the
 # stage return at once).
 STAGE_KERNEL = {"sort_gather": ("k_csort_clear", "k_csort_count", "k_csort"),
-                "build_ngh": ("k_cell_prep",), "border_assign": ("k_labels",)}
+                "build_ngh": ("k_cell_prep",), "core_mark": ("k_core",),
+                "border_assign": ("k_labels",)}
 PROFILE_MD = os.path.join(ROOT, "profiles", "kernels_constant_density_10M.md")
+
+
+def _synthetic():
+    """The seeded generators (dbscan_torch/synthetic.py), loaded from their
+    file so that nothing of the package -- in particular its native
+    extension -- is imported (the reference arm must load the reference
+    only)."""
+    mod = sys.modules.get("dbs_bench_synthetic")
+    if mod is None:
+        path = os.path.join(PKG_DIR, "dbscan_torch", "synthetic.py")
+        spec = importlib.util.spec_from_file_location("dbs_bench_synthetic", path)
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        sys.modules["dbs_bench_synthetic"] = mod
+    return mod
+
+
+def _package():
+    if PKG_DIR not in sys.path:
+        sys.path.insert(0, PKG_DIR)
+    import dbscan_torch
+    return dbscan_torch
+
+
+def base_config(world: int) -> dict:
+    """The workload, identical in both arms' lines."""
+    return {"workload": WORKLOAD, "n_points": N_POINTS, "eps": EPS, "min_samples": MIN_SAMPLES,
+            "parallelism": "replicas" if world > 1 else "single",
+            "l2": "inputs larger than L2 (80 MB points, 40 MB labels, ~3.4 GB of pipeline arrays); "
+                  "the GPU arm also writes a 512 MB buffer between timed steps, outside the events"}
 
 
 def _peaks():
@@ -100,7 +142,6 @@ class ClockSampler:
         self._file = None
 
     def __enter__(self):
-        import tempfile
         self._file = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
         try:
             self._proc = subprocess.Popen(
@@ -203,10 +244,12 @@ def ncu_traffic(kernels):
     return int(round(sum(found.values())))
 
 
+# ------------------------------------------------------------ baseline legs
 def cpu_baseline(X: np.ndarray, eps: float, ms: int, budget_s: float = 15.0):
     """The reference's CPU path (oracle/_ref/cpu) on all host cores, else the
     single-threaded C oracle port; bounded to ~budget_s of CPU work."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    if ORACLE_DIR not in sys.path:
+        sys.path.insert(0, ORACLE_DIR)
     import refmod
     ref = refmod.load("cpu")
     cores = os.cpu_count() or 1
@@ -233,9 +276,74 @@ def cpu_baseline(X: np.ndarray, eps: float, ms: int, budget_s: float = 15.0):
     med = statistics.median(times)
     return {"value": round(X.shape[0] / med / 1e6, 3), "unit": UNIT, "cores": used, "kind": kind,
             "sample": f"{len(times)} calls on the full {X.shape[0]:,}-point workload, median "
-                      f"{med * 1e3:.1f} ms/call ({cores} host cores visible)"}
+                      f"{med * 1e3:.1f} ms/call ({cores} host cores visible; fresh process, no GPU work)"}
 
 
+def reference_cuda_leg(X_np: np.ndarray, steps: int, warmup: int, labels_out: str):
+    """The reference's CUDA build (oracle/_ref/cuda) timed like this build:
+    W warm-up calls, then `steps` calls each bracketed by CUDA events on the
+    current stream, a 512 MB buffer written between calls outside the events;
+    plus the median of three dbscan2d_profile stage splits. Labels of the last
+    call go to `labels_out` (.npy) for the parent to compare."""
+    if ORACLE_DIR not in sys.path:
+        sys.path.insert(0, ORACLE_DIR)
+    import refmod
+    ref = refmod.load("cuda")
+    if ref is None:
+        return {"unavailable": "reference CUDA build not present in oracle/_ref/cuda"}
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    X = torch.from_numpy(X_np).to(dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    lab = None
+    for _ in range(max(3, warmup)):
+        lab = ref.dbscan2d(X, EPS, MIN_SAMPLES)
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for k in range(steps):
+        flush.fill_(float(k))
+        ev[k][0].record(stream)
+        lab = ref.dbscan2d(X, EPS, MIN_SAMPLES)
+        ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    ms = [a.elapsed_time(b) for a, b in ev]
+    profs = []
+    for k in range(3):
+        flush.fill_(float(k))
+        profs.append(ref.dbscan2d_profile(X, EPS, MIN_SAMPLES)[1])
+    stage = {s: round(statistics.median(p[s] for p in profs), 4) for s in profs[0]}
+    np.save(labels_out, lab.cpu().numpy())
+    mean = sum(ms) / len(ms)
+    return {"ms_per_step": round(mean, 4), "median_ms": round(statistics.median(ms), 4),
+            "value": round(X_np.shape[0] / (mean * 1e-3) / 1e6, 2), "unit": UNIT, "steps": steps,
+            "stage_ms": stage,
+            "build": "reference csrc/ (extension.cpp, cpu/dbscan_cpu.cpp, cuda/dbscan_cuda.cu) built "
+                     "by oracle/build_ref.py: nvcc -O3 --use_fast_math, TORCH_CUDA_ARCH_LIST=10.0"}
+
+
+def _child_leg(leg: str, points: str, extra=()) -> dict:
+    """Runs one baseline leg of this script in a fresh child process and
+    returns its JSON line (or an object saying why there is none)."""
+    cmd = [sys.executable, os.path.abspath(__file__), "--leg", leg, "--points-file", points, *extra]
+    try:
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=900)
+    except subprocess.TimeoutExpired:
+        return {"unavailable": f"{leg} leg timed out"}
+    for line in reversed(r.stdout.splitlines()):
+        if line.startswith("{"):
+            return json.loads(line)
+    return {"unavailable": f"{leg} leg exited {r.returncode}: {r.stderr.strip()[-300:]}"}
+
+
+def run_leg(args):
+    X = np.load(args.points_file)
+    if args.leg == "cpu":
+        return cpu_baseline(X, EPS, MIN_SAMPLES)
+    return reference_cuda_leg(X, args.steps, args.warmup, args.labels_out)
+
+
+# ------------------------------------------------------------------- setup
 def dist_setup(n_gpus: int):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -246,8 +354,6 @@ def dist_setup(n_gpus: int):
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
-    elif torch.cuda.is_available():
-        torch.cuda.set_device(0)
     return world, rank, local
 
 
@@ -267,33 +373,53 @@ def max_over_ranks(v: float, world: int) -> float:
     return float(t.item())
 
 
+# ---------------------------------------------------------- reference arm
 def run_reference(args, world, rank):
-    from dbscan_torch import synthetic
+    """The reference's own CPU implementation on this workload: imports the
+    generators (by file) and the reference's module, nothing of this build."""
     if rank != 0:
         return None
-    X = synthetic.constant_density(N_POINTS, seed=0)
+    X = _synthetic().constant_density(N_POINTS, seed=0)
     base = cpu_baseline(X, EPS, MIN_SAMPLES, budget_s=max(10.0, 2.0 * args.steps))
     return {"metric": METRIC, "value": base["value"], "unit": UNIT, "impl": "reference",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(N_POINTS / (base["value"] * 1e6) * 1e3, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded constant-density Gaussian blobs + 2% noise)",
-            "config": {"workload": WORKLOAD, "n_points": N_POINTS, "eps": EPS,
-                       "min_samples": MIN_SAMPLES, "device": "host CPU"},
+            "data": DATA, "config": base_config(world), "device": "host CPU",
             "cpu_baseline": base,
             "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
 
 
+# ----------------------------------------------------------------- our arm
 def run_ours(args, world, rank, local):
-    from dbscan_torch import _C, dbscan2d, synthetic
+    syn = _synthetic()
+    X_np = syn.constant_density(N_POINTS, seed=rank)
+
+    # Baseline legs first, each in a fresh child process, before this process
+    # touches the GPU or loads this build.
+    legs = {}
+    tmpdir = None
+    if rank == 0 and world == 1 and not (args.no_cpu_baseline and args.no_reference_cuda):
+        tmpdir = tempfile.mkdtemp(prefix="dbs_bench_")
+        pts = os.path.join(tmpdir, "points.npy")
+        np.save(pts, X_np)
+        if not args.no_cpu_baseline:
+            legs["cpu"] = _child_leg("cpu", pts)
+        if not args.no_reference_cuda:
+            legs["ref_cuda"] = _child_leg("ref_cuda", pts, ["--steps", str(args.steps), "--warmup",
+                                                            str(args.warmup), "--labels-out",
+                                                            os.path.join(tmpdir, "ref_labels.npy")])
+
+    torch.cuda.set_device(local)
+    pkg = _package()
+    _C, dbscan2d = pkg._C, pkg.dbscan2d
     dev = torch.device("cuda", local)
-    X_np = synthetic.constant_density(N_POINTS, seed=rank)
     X = torch.from_numpy(X_np).to(dev)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
 
-    # Shape of the pipeline on this input (cells, key width, passes).
+    # Shape and work counts of the pipeline on this input.
     _, info = _C.dbscan2d_info(X, EPS, MIN_SAMPLES)
     # Warm-up as the timed loop runs: each result held until the next call
     # returns, so both label buffers the loop alternates between have their
@@ -322,6 +448,7 @@ def run_ours(args, world, rank, local):
     ms_mean = sum(step_ms) / len(step_ms)
     ms_max = max_over_ranks(ms_mean, world)
     value = world * N_POINTS / (ms_max * 1e-3) / 1e6
+    ours_labels = labels.cpu().numpy()
 
     # Per-stage split (profile entry point: CUDA events between stages).
     prof_runs = []
@@ -373,19 +500,29 @@ def run_ours(args, world, rank, local):
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max, 4),
            "step_ms": step_stats,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-           "data": "synthetic (seeded constant-density Gaussian blobs + 2% noise)",
-           "config": {"workload": WORKLOAD, "n_points": N_POINTS, "eps": EPS,
-                      "min_samples": MIN_SAMPLES, "parallelism": "replicas" if world > 1 else "single",
-                      "l2": "flushed between steps (512 MB write outside the timed events)",
-                      "num_cells": cells, "key_bits": info["key_bits"], "radix_passes": passes,
-                      "sort": "counting" if passes == 0 else "radix"},
+           "data": DATA, "config": base_config(world),
+           "pipeline": {"num_cells": cells, "key_bits": info["key_bits"], "radix_passes": passes,
+                        "sort": "counting" if passes == 0 else "radix",
+                        "queries": info["queries"], "border_points": info["border"],
+                        "union_pairs": [info["pairs_ring0"], info["pairs_ring1"]],
+                        "union_warp_pairs": [info["warp_pairs_ring0"], info["warp_pairs_ring1"]]},
            "clocks": clocks.summary(),
            "e2e": {"value": round(world * N_POINTS / (e2e_mean * 1e-3) / 1e6, 2), "unit": UNIT,
                    "h2d_bytes_per_step": N_POINTS * 8, "d2h_bytes_per_step": N_POINTS * 4},
            "gpu_launches": KERNELS_PER_CALL * args.steps,
            "roofline": roof}
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        out["cpu_baseline"] = cpu_baseline(X_np, EPS, MIN_SAMPLES)
+    if "cpu" in legs:
+        out["cpu_baseline"] = legs["cpu"]
+    if "ref_cuda" in legs:
+        rc = legs["ref_cuda"]
+        if "ms_per_step" in rc:
+            ref_lab = np.load(os.path.join(tmpdir, "ref_labels.npy"))
+            rc["labels_equal"] = bool(np.array_equal(ref_lab, ours_labels))
+            rc["speedup"] = round(rc["ms_per_step"] / ms_mean, 2)
+        out["reference_cuda"] = rc
+    if tmpdir is not None:
+        import shutil
+        shutil.rmtree(tmpdir, ignore_errors=True)
     del labels, X, flush, X_host
     torch.cuda.empty_cache()
     if world == 1:
@@ -394,7 +531,7 @@ def run_ours(args, world, rank, local):
         if args.batched_clouds > 0:
             out["batched"] = run_batched(dev, args.batched_clouds)
         if args.serve_seconds > 0:
-            out["serving"] = run_serving(dev, args.serve_seconds)
+            out["serving"] = run_serving(dev, args.serve_seconds, args.serve_sweep_seconds)
     elif args.batched_clouds > 0:
         out["batched"] = run_batched_sharded(dev, args.batched_clouds, world, rank)
     return out
@@ -410,27 +547,17 @@ def _ev_ms(fn):
     return a.elapsed_time(b), out
 
 
-def batch_config(n_clouds: int):
-    """Sizes (log-uniform in [256, 262144]), eps_i in [0.2, 1.0] and
-    min_samples_i in {4..32} of the batched workload, seeded."""
-    rng = np.random.default_rng(0)
-    sizes = np.exp(rng.uniform(np.log(256), np.log(262_144), size=n_clouds)).astype(np.int64)
-    eps = rng.uniform(0.2, 1.0, size=n_clouds)
-    ms = rng.integers(4, 33, size=n_clouds)
-    return sizes, eps, ms
-
-
 def run_batched_sharded(dev, n_clouds: int, world: int, rank: int) -> dict:
     """The batched workload split across ranks by shard_clouds (independent
     clouds, no collective on the data path): each rank clusters its shard in
     one batched run; the time is the max over ranks."""
-    from dbscan_torch import dbscan2d_batched, shard_clouds, synthetic
-    sizes, eps, ms = batch_config(n_clouds)
-    mine = shard_clouds(sizes, world)[rank]
-    X, off = synthetic.blobs_with_noise_device(sizes[mine], seed=rank, device=dev)
-    dbscan2d_batched(X, off, eps[mine], ms[mine])  # warm-up
-    tb = [_ev_ms(lambda: dbscan2d_batched(X, off, eps[mine], ms[mine]))[0] for _ in range(3)]
-    _C_check()
+    pkg = _package()
+    sizes, eps, ms = _synthetic().batch_layout(n_clouds, seed=0)
+    mine = pkg.shard_clouds(sizes, world)[rank]
+    X, off = _synthetic().blobs_with_noise_device(sizes[mine], seed=rank, device=dev)
+    pkg.dbscan2d_batched(X, off, eps[mine], ms[mine])  # warm-up
+    tb = [_ev_ms(lambda: pkg.dbscan2d_batched(X, off, eps[mine], ms[mine]))[0] for _ in range(3)]
+    pkg.check_status()
     t = max_over_ranks(statistics.median(tb), world)
     del X
     torch.cuda.empty_cache()
@@ -447,9 +574,10 @@ def run_batched(dev, n_clouds: int) -> dict:
     clouds. Both timed with CUDA events; labels compared cloud by cloud.
     Then the same batch through a BatchedPlan (CUDA graph replay) with the
     built-in launch shape and with the shape BatchedPlan.tune() picks."""
-    from dbscan_torch import BatchedPlan, dbscan2d, dbscan2d_batched, synthetic
-    sizes, eps, ms = batch_config(n_clouds)
-    X, off = synthetic.blobs_with_noise_device(sizes, seed=0, device=dev)
+    pkg = _package()
+    dbscan2d, dbscan2d_batched = pkg.dbscan2d, pkg.dbscan2d_batched
+    sizes, eps, ms = _synthetic().batch_layout(n_clouds, seed=0)
+    X, off = _synthetic().blobs_with_noise_device(sizes, seed=0, device=dev)
     offl = off.tolist()
     dbscan2d_batched(X, off, eps, ms)  # warm-up
     tb = []
@@ -463,10 +591,10 @@ def run_batched(dev, n_clouds: int) -> dict:
     loop()  # warm-up: the caching allocator holds every workspace size afterwards
     tp, labs = _ev_ms(loop)
     equal = all(torch.equal(labs[k], lab_b[offl[k]:offl[k + 1]]) for k in range(n_clouds))
-    _C_check()
+    pkg.check_status()
     del labs
     torch.cuda.empty_cache()
-    plan = BatchedPlan(offl)
+    plan = pkg.BatchedPlan(offl)
     plan.run(X, eps, ms)  # captures the graph (built-in shape)
     t_plan = statistics.median([_ev_ms(plan.run)[0] for _ in range(3)])
     t0 = time.perf_counter()
@@ -501,11 +629,13 @@ def run_configs(dev) -> dict:
     call (median of 7 after 3 warm-ups): config 0 (100k blobs with noise),
     config 1 at 1M and 5M points, config 2 (adversarial 4M cloud, min_samples
     4 and 32)."""
-    from dbscan_torch import dbscan2d, synthetic
-    cases = [("blobs_100k", lambda: synthetic.blobs_with_noise(100_000, seed=0), 0.5, 10),
-             ("constant_density_1M", lambda: synthetic.constant_density(1_000_000, seed=0), 0.5, 10),
-             ("constant_density_5M", lambda: synthetic.constant_density(5_000_000, seed=0), 0.5, 10),
-             ("adversarial_4M_ms4", lambda: synthetic.adversarial(4_000_000, seed=0), 0.5, 4),
+    pkg = _package()
+    syn = _synthetic()
+    dbscan2d = pkg.dbscan2d
+    cases = [("blobs_100k", lambda: syn.blobs_with_noise(100_000, seed=0), 0.5, 10),
+             ("constant_density_1M", lambda: syn.constant_density(1_000_000, seed=0), 0.5, 10),
+             ("constant_density_5M", lambda: syn.constant_density(5_000_000, seed=0), 0.5, 10),
+             ("adversarial_4M_ms4", lambda: syn.adversarial(4_000_000, seed=0), 0.5, 4),
              ("adversarial_4M_ms32", None, 0.5, 32)]
     out = {}
     X = None
@@ -518,38 +648,46 @@ def run_configs(dev) -> dict:
         t = statistics.median(ts)
         out[name] = {"n_points": int(X.shape[0]), "eps": eps, "min_samples": ms, "ms": round(t, 4),
                      "mpoints_per_s": round(X.shape[0] / (t * 1e-3) / 1e6, 1)}
-    _C_check()
+    pkg.check_status()
     del X
     torch.cuda.empty_cache()
     return out
 
 
-def _C_check():
-    from dbscan_torch import check_status
-    check_status()
+# ----------------------------------------------------------------- serving
+SERVE_RATE_HZ = 2000.0
+SERVE_BUDGET = 64 << 30
+P99_BOUND_MS = 50.0
 
 
-def run_serving(dev, seconds: float, rate_hz: float = 2000.0, budget_bytes: int = 64 << 30) -> dict:
-    """Config 4: Poisson arrivals at rate_hz for `seconds`, sizes log-uniform in
-    [1e3, 2e6] (prefixes of shuffled 2M-point clouds of the config-0
-    distribution, pinned on the host), eps U[0.1, 1.0], min_samples U{4..32}.
-    The continuous-batching server (64 GiB admission budget) against
-    sequential plain calls on the same stream; latency = completion minus
-    arrival, host clock."""
-    from dbscan_torch import DbscanServer, dbscan2d, synthetic
-    arrivals, sizes, eps, ms, _ = synthetic.request_stream(rate_hz=rate_hz, duration_s=seconds, seed=0)
-    pool_n, pool_k = 2_000_000, 8
-    pool_d, pool_off = synthetic.blobs_with_noise_device([pool_n] * pool_k, seed=1, device=dev)
-    pool = pool_d.cpu().pin_memory()
-    del pool_d
-    reqs_x = [pool[int(pool_off[k % pool_k]): int(pool_off[k % pool_k]) + int(sizes[k])]
-              for k in range(len(sizes))]
-    n = len(reqs_x)
+class RequestPool:
+    """Host-side request clouds of the config-0 distribution: `bases` clouds
+    of `base_n` points (20 blobs + 5% noise, shuffled; device generator, one
+    seed per cloud) copied once to pinned host memory. Request i is the
+    window of its size at a seeded random offset of base cloud i mod bases:
+    a random subsample of a shuffled config-0 cloud, so a config-0 cloud of
+    that size, and no two requests share their point set."""
 
-    srv = DbscanServer(budget_bytes=budget_bytes, lane_points=16 << 20, lane_clouds=256)
-    for k in range(8):  # warm-up batch
-        srv.submit(reqs_x[k], float(eps[k]), int(ms[k]))
-    srv.drain()
+    def __init__(self, dev, bases: int = 64, base_n: int = 2_000_000, seed: int = 1):
+        X, _ = _synthetic().blobs_with_noise_device([base_n] * bases, seed=seed, device=dev)
+        self.host = X.cpu().pin_memory()
+        del X
+        torch.cuda.empty_cache()
+        self.bases, self.base_n = bases, base_n
+
+    def windows(self, sizes, seed):
+        rng = np.random.default_rng(seed)
+        off = rng.integers(0, self.base_n - np.asarray(sizes) + 1)
+        return [self.host[(i % self.bases) * self.base_n + int(o):
+                          (i % self.bases) * self.base_n + int(o) + int(n)]
+                for i, (o, n) in enumerate(zip(off, sizes))]
+
+
+def _serve(srv, xs, arrivals, eps, ms):
+    """Offers the requests to the server at their arrival times (host
+    clock); returns (latencies ms, clouds/s from the first arrival to the last
+    completion, batches)."""
+    n = len(xs)
     srv.batches = srv.completed = 0
     reqs = []
     t0 = time.perf_counter()
@@ -557,41 +695,106 @@ def run_serving(dev, seconds: float, rate_hz: float = 2000.0, budget_bytes: int 
     while i < n or srv.queue or any(l.busy for l in srv.lanes):
         now = time.perf_counter() - t0
         while i < n and arrivals[i] <= now:
-            reqs.append(srv.submit(reqs_x[i], float(eps[i]), int(ms[i]), t_submit=t0 + arrivals[i]))
+            reqs.append(srv.submit(xs[i], float(eps[i]), int(ms[i]), t_submit=t0 + arrivals[i]))
             i += 1
         if srv.step() == 0:
             time.sleep(20e-6)
     t_end = max(r.t_done for r in reqs) - t0
-    lat_s = np.array([r.latency for r in reqs]) * 1e3
+    return np.array([r.latency for r in reqs]) * 1e3, n / t_end, srv.batches, reqs
 
-    for k in range(8):  # warm-up of the plain path
-        dbscan2d(reqs_x[k], float(eps[k]), int(ms[k]))
-    lat_p = np.empty(n)
-    sample = {}
+
+def _plain(dbscan2d, xs, arrivals, eps, ms, keep_every=0):
+    """Sequential plain calls (CPU tensor in, labels back on the host) in
+    arrival order, each started at its arrival time or when the previous one
+    finished; returns (latencies ms, clouds/s, kept labels)."""
+    n = len(xs)
+    lat = np.empty(n)
+    kept = {}
     t0 = time.perf_counter()
     for k in range(n):
         while time.perf_counter() - t0 < arrivals[k]:
             pass
-        lab = dbscan2d(reqs_x[k], float(eps[k]), int(ms[k]))
-        lat_p[k] = (time.perf_counter() - t0 - arrivals[k]) * 1e3
-        if k % 97 == 0:
-            sample[k] = lab
-    t_end_p = time.perf_counter() - t0
-    equal = all(torch.equal(reqs[k].labels, lab) for k, lab in sample.items())
-    batches = srv.batches
-    del pool, reqs_x, reqs, srv
+        lab = dbscan2d(xs[k], float(eps[k]), int(ms[k]))
+        lat[k] = (time.perf_counter() - t0 - arrivals[k]) * 1e3
+        if keep_every and k % keep_every == 0:
+            kept[k] = lab
+    return lat, n / (time.perf_counter() - t0), kept
+
+
+def _pct(a, q):
+    return round(float(np.percentile(a, q)), 3)
+
+
+def run_serving(dev, seconds: float, sweep_seconds: float) -> dict:
+    """Config 4: Poisson arrivals at 2,000 req/s for `seconds`, sizes
+    log-uniform in [1e3, 2e6] (config-0 clouds), eps U[0.1, 1.0], min_samples
+    U{4..32}, through the continuous-batching server (admission under a 64 GiB
+    budget, checked against free device memory) and through sequential plain
+    calls; latency = completion minus arrival (host clock). Then a saturation
+    sweep per arm: offered rates rising by sqrt(2) from 1,000 req/s, each for
+    `sweep_seconds`, until p99 exceeds 50 ms or the arm falls behind (achieved
+    below 95% of offered); the arm's capacity is the highest offered rate that
+    stayed within both."""
+    pkg = _package()
+    syn = _synthetic()
+    pool = RequestPool(dev)
+    free0, total = torch.cuda.mem_get_info(dev)
+    srv = pkg.DbscanServer(budget_bytes=SERVE_BUDGET, lane_points=16 << 20, lane_clouds=256)
+
+    def stream(rate, dur, seed):
+        arr, sizes, eps, ms, _ = syn.request_stream(rate_hz=rate, duration_s=dur, seed=seed)
+        return arr, pool.windows(sizes, seed + 7), eps, ms, sizes
+
+    # Warm-up of both arms.
+    arr, xs, eps, ms, _ = stream(200.0, 0.2, 99)
+    _serve(srv, xs, arr, eps, ms)
+    for k in range(min(8, len(xs))):
+        pkg.dbscan2d(xs[k], float(eps[k]), int(ms[k]))
+
+    arr, xs, eps, ms, sizes = stream(SERVE_RATE_HZ, seconds, 0)
+    lat_s, cps_s, batches, reqs = _serve(srv, xs, arr, eps, ms)
+    lat_p, cps_p, kept = _plain(pkg.dbscan2d, xs, arr, eps, ms, keep_every=97)
+    equal = all(torch.equal(reqs[k].labels, lab) for k, lab in kept.items())
+    del reqs, kept
+
+    def sweep(run_arm):
+        steps = []
+        rate = 1000.0
+        while rate <= 64000.0:
+            a, x, e, m, _ = stream(rate, sweep_seconds, int(rate))
+            lat, cps = run_arm(x, a, e, m)
+            ok = _pct(lat, 99) <= P99_BOUND_MS and cps >= 0.95 * len(x) / max(a[-1], 1e-9)
+            steps.append({"offered": round(rate), "achieved": round(cps, 1), "p50_ms": _pct(lat, 50),
+                          "p99_ms": _pct(lat, 99), "ok": bool(ok)})
+            if not ok:
+                break
+            rate *= 2 ** 0.5
+        good = [s for s in steps if s["ok"]]
+        return {"capacity_clouds_per_s": good[-1]["achieved"] if good else 0.0,
+                "capacity_offered": good[-1]["offered"] if good else 0, "steps": steps}
+
+    srv_arena = srv.arena_bytes
+    sat_s = sweep(lambda x, a, e, m: _serve(srv, x, a, e, m)[:2])
+    sat_p = sweep(lambda x, a, e, m: _plain(pkg.dbscan2d, x, a, e, m)[:2])
+    pkg.check_status()
+    del pool, srv
     torch.cuda.empty_cache()
-    pct = lambda a, q: round(float(np.percentile(a, q)), 3)
-    return {"workload": f"Poisson {rate_hz:g} req/s for {seconds:g} s, N log-uniform [1e3, 2e6], "
+    ratio = (sat_s["capacity_clouds_per_s"] / sat_p["capacity_clouds_per_s"]
+             if sat_p["capacity_clouds_per_s"] else None)
+    return {"workload": f"Poisson {SERVE_RATE_HZ:g} req/s for {seconds:g} s, N log-uniform [1e3, 2e6] "
+                        f"(config-0 clouds: windows at random offsets of 64 shuffled 2M-point clouds), "
                         f"eps U[0.1, 1.0], min_samples U{{4..32}}",
-            "requests": n, "mean_points": round(float(np.mean(sizes)), 1),
-            "budget_gb": round(budget_bytes / 2**30, 1), "arena_gb": round(
-                (2 * __import__("dbscan_torch").footprint_bytes(16 << 20, 256)) / 2**30, 2),
-            "server": {"p50_ms": pct(lat_s, 50), "p99_ms": pct(lat_s, 99),
-                       "clouds_per_s": round(n / t_end, 1), "batches": batches},
-            "sequential_plain": {"p50_ms": pct(lat_p, 50), "p99_ms": pct(lat_p, 99),
-                                 "clouds_per_s": round(n / t_end_p, 1)},
-            "labels_equal_sampled": bool(equal)}
+            "requests": len(xs), "mean_points": round(float(np.mean(sizes)), 1),
+            "budget_gb": round(SERVE_BUDGET / 2**30, 1), "free_hbm_gb": round(free0 / 2**30, 1),
+            "arena_gb": round(srv_arena / 2**30, 2),
+            "server": {"p50_ms": _pct(lat_s, 50), "p99_ms": _pct(lat_s, 99),
+                       "clouds_per_s": round(cps_s, 1), "batches": batches},
+            "sequential_plain": {"p50_ms": _pct(lat_p, 50), "p99_ms": _pct(lat_p, 99),
+                                 "clouds_per_s": round(cps_p, 1)},
+            "labels_equal_sampled": bool(equal),
+            "saturation": {"p99_bound_ms": P99_BOUND_MS, "step_seconds": sweep_seconds,
+                           "server": sat_s, "sequential_plain": sat_p,
+                           "capacity_ratio": round(ratio, 2) if ratio else None}}
 
 
 def main():
@@ -601,13 +804,23 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-reference-cuda", action="store_true",
+                    help="skip the timing of the reference's CUDA build")
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the timings of the other plain-call workloads")
     ap.add_argument("--batched-clouds", type=int, default=4096,
                     help="clouds of the batched comparison (0 skips it)")
-    ap.add_argument("--serve-seconds", type=float, default=10.0,
-                    help="length of the serving stream (0 skips it)")
+    ap.add_argument("--serve-seconds", type=float, default=60.0,
+                    help="length of the config-4 serving stream (0 skips serving)")
+    ap.add_argument("--serve-sweep-seconds", type=float, default=3.0,
+                    help="length of each offered-rate step of the saturation sweep")
+    ap.add_argument("--leg", choices=["cpu", "ref_cuda"], help=argparse.SUPPRESS)
+    ap.add_argument("--points-file", help=argparse.SUPPRESS)
+    ap.add_argument("--labels-out", help=argparse.SUPPRESS)
     args = ap.parse_args()
+    if args.leg:
+        print(json.dumps(run_leg(args)), flush=True)
+        return
     world, rank, local = dist_setup(args.gpus)
     try:
         if args.impl == "reference":

@@ -90,6 +90,8 @@ def build_ext(force: bool = False, verbose: bool = True) -> str:
     existing = glob.glob(os.path.join(PKG, "_C*.so"))
     deps = [src, os.path.join(INCLUDE, "dbscan_b200.h"), LIB]
     if existing and not force and not _newer(existing[0], deps):
+        if not os.path.exists(os.path.join(PKG, "_build_info.py")):
+            write_build_info()
         return existing[0]
     tmp = os.path.join(BUILD, "ext")
     os.makedirs(tmp, exist_ok=True)
@@ -113,7 +115,20 @@ def build_ext(force: bool = False, verbose: bool = True) -> str:
         os.remove(old)
     dst = os.path.join(PKG, "_C.so")
     shutil.copy2(built[0], dst)
+    write_build_info()
     return dst
+
+
+def write_build_info() -> str:
+    """Stamps the torch version the extension was built against into
+    dbscan_torch/_build_info.py; the package refuses to import against another
+    torch minor version (the extension's C++ ABI is tied to it)."""
+    import torch
+    path = os.path.join(PKG, "_build_info.py")
+    with open(path, "w") as f:
+        f.write('"""Written by build.py: the torch version the native extension was built against."""\n')
+        f.write(f"BUILD_TORCH_VERSION = {torch.__version__!r}\n")
+    return path
 
 
 def main(argv=None) -> int:

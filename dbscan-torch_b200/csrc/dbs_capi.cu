@@ -293,13 +293,22 @@ int dbs_dbscan2d_profile(const float* X, int64_t n, double eps, int64_t min_samp
 int dbs_dbscan2d_debug(const float* X, int64_t n, double eps, int64_t min_samples,
                        int32_t* labels, void* ws, size_t ws_bytes, void* stream,
                        const dbs_debug_buffers* out, int64_t* num_cells) {
-  if (out == nullptr || num_cells == nullptr) return DBS_ERR_INVALID;
+  return dbs_dbscan2d_debug_ex(X, n, eps, min_samples, labels, ws, ws_bytes, stream, out, num_cells,
+                               DBS_DEBUG_STABLE_SORT);
+}
+
+int dbs_dbscan2d_debug_ex(const float* X, int64_t n, double eps, int64_t min_samples,
+                          int32_t* labels, void* ws, size_t ws_bytes, void* stream,
+                          const dbs_debug_buffers* out, int64_t* num_cells, int32_t flags) {
+  if (out == nullptr || num_cells == nullptr || (flags & ~DBS_DEBUG_STABLE_SORT) != 0)
+    return DBS_ERR_INVALID;
   *num_cells = 0;
   Plan p;
   int rc = prepare_single(X, n, eps, min_samples, labels, ws, ws_bytes, &p);
   if (rc != DBS_OK || n == 0) return rc;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  p.force_radix = 1;  // stable sort: perm and sorted coordinates as the reference's
+  // Stable sort: perm and sorted coordinates as the reference's.
+  p.force_radix = (flags & DBS_DEBUG_STABLE_SORT) ? 1 : 0;
   rc = run_pipeline(p, s, nullptr);
   if (rc != DBS_OK) return rc;
   rc = run_debug_export(p, *out, s, n);
@@ -472,6 +481,29 @@ int dbs_read_plan(const void* ws, void* stream, int64_t* num_cells, int32_t* key
   if (key_bits) *key_bits = (int32_t)h.nbits;
   if (passes) *passes = h.dense_sort ? 0 : (int32_t)h.npasses;
   if (key_bytes) *key_bytes = h.key64 ? 8 : 4;
+  return DBS_OK;
+}
+
+int dbs_read_stats(const void* ws, void* stream, dbs_run_stats* out) {
+  if (ws == nullptr || out == nullptr) return DBS_ERR_INVALID;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  Desc h;
+  if (cudaMemcpyAsync(&h, ws, sizeof(Desc), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return DBS_ERR_CUDA;
+  out->num_cells = h.num_cells;
+  out->key_bits = (int32_t)h.nbits;
+  out->passes = h.dense_sort ? 0 : (int32_t)h.npasses;
+  out->key_bytes = h.key64 ? 8 : 4;
+  out->hot_slots = (int32_t)h.hot_used;
+  out->queries = h.q_count;
+  out->border = h.b_count;
+  // The flatten between the passes saved pass 0's counts; pass 1's are the
+  // live counters.
+  out->pairs[0] = h.ring_pairs[0];
+  out->pairs[1] = h.p_count;
+  out->warp_pairs[0] = h.ring_warp[0];
+  out->warp_pairs[1] = h.d_count;
   return DBS_OK;
 }
 

@@ -354,7 +354,10 @@ __global__ void __launch_bounds__(256) k_pair_warp(Plan p) {
 __global__ void __launch_bounds__(256) k_flatten(Plan p) {
   Desc* d = p.desc;
   const uint32_t C = d->num_cells;
-  if (blockIdx.x == 0 && threadIdx.x == 0) { d->p_count = 0; d->d_count = 0; }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    d->ring_pairs[0] = d->p_count; d->ring_warp[0] = d->d_count;
+    d->p_count = 0; d->d_count = 0;
+  }
   for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < C; c += gridDim.x * blockDim.x)
     p.uf[c] = uf_find_ro(p.uf, (int32_t)c, d);
 }

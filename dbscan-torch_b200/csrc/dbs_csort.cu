@@ -119,7 +119,10 @@ __device__ __forceinline__ int hot_insert(const Plan& p, uint32_t key) {
   uint32_t s = hot_hash(key);
   for (int probe = 0; probe < kHotProbes; ++probe, s = (s + 1) & (kHotSlots - 1)) {
     uint32_t k = __ldcg(&p.hot_key[s]);
-    if (k == kHotEmpty) k = atomicCAS(&p.hot_key[s], kHotEmpty, key);  // the slot's old value
+    if (k == kHotEmpty) {
+      k = atomicCAS(&p.hot_key[s], kHotEmpty, key);  // the slot's old value
+      if (k == kHotEmpty) atomicAdd(&p.desc->hot_used, 1u);  // this lane took the slot
+    }
     if (k == kHotEmpty || k == key) return (int)s;
   }
   return -1;
@@ -467,12 +470,12 @@ __global__ void __launch_bounds__(kCsThreads, 5) k_csort(Plan p) {
 }
 
 cudaError_t launch_csort(const Plan& p, cudaStream_t s) {
-  static int blocks_per_sm = 0;
-  if (blocks_per_sm == 0) {
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_csort, kCsThreads, 0);
-    if (e != cudaSuccess) return e;
-    if (blocks_per_sm < 1) return cudaErrorLaunchOutOfResources;
-  }
+  static PerDeviceBlocks cache;
+  int blocks_per_sm = 0;
+  cudaError_t e = cache.get(
+      [](int* b) { return cudaOccupancyMaxActiveBlocksPerMultiprocessor(b, k_csort, kCsThreads, 0); },
+      &blocks_per_sm);
+  if (e != cudaSuccess) return e;
   k_csort_clear<<<p.num_sms * 4, kCsThreads, 0, s>>>(p);
   k_csort_count<<<p.num_sms * p.bps[kTuneCount], kCsThreads, 0, s>>>(p);
   int grid = p.num_sms * blocks_per_sm;

@@ -29,6 +29,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <mutex>
+
 namespace dbs {
 
 constexpr int kRadixBits = 8;
@@ -164,7 +166,9 @@ struct Desc {
   uint32_t b_count;     // border list length (non-core points)
   uint32_t p_count;     // union-find candidate pair list length
   uint32_t d_count;     // pairs deferred to warp-cooperative scans
-  uint32_t pad1;
+  uint32_t hot_used;    // counting sort: occupied hot-key slots
+  uint32_t ring_pairs[2];  // p_count of each union pass (kept for the stats read-back)
+  uint32_t ring_warp[2];   // d_count of each union pass
   GridBar bar;
   // %globaltimer (ns) at each phase boundary of the cooperative kernels,
   // written by block 0 after each grid barrier: a per-phase split readable
@@ -408,6 +412,34 @@ __device__ __forceinline__ void grid_sync(GridBar* b, Desc* d) {
 }
 
 // --------------------------------------------------------- host launchers
+// One-time set-up of a cooperative kernel on the current device (dynamic
+// shared-memory attribute, resident blocks per SM). Kernel attributes belong
+// to a device, so the result is cached per device ordinal: a process that
+// runs on cuda:0 and then on cuda:1 sets the attribute on both. `setup(&b)`
+// sets the attributes and stores the resident blocks per SM in b. The mutex
+// serialises host threads that launch at the same time.
+constexpr int kMaxDevices = 64;
+struct PerDeviceBlocks {
+  std::mutex mu;
+  int blocks[kMaxDevices] = {0};
+  template <typename F>
+  cudaError_t get(F setup, int* out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(mu);
+    if (blocks[dev] == 0) {
+      int b = 0;
+      if ((e = setup(&b)) != cudaSuccess) return e;
+      if (b < 1) return cudaErrorLaunchOutOfResources;
+      blocks[dev] = b;
+    }
+    *out = blocks[dev];
+    return cudaSuccess;
+  }
+};
+
 // Each returns cudaGetLastError() of its launches.
 cudaError_t launch_front(const Plan& p, cudaStream_t s);      // init, bounds, finalize, keys
 cudaError_t launch_keys(const Plan& p, cudaStream_t s);

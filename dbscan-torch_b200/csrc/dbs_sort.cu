@@ -41,7 +41,11 @@ __global__ void k_init(Plan p) {
     d->big_packed = 0;
   }
   for (int64_t i = tid; i < 2 * kRadix; i += stride) (&d->digit_total[0][0])[i] = 0;
-  if (tid == 0) { d->bar.count = 0; d->bar.gen = 0; d->dense_sort = 0; d->q_count = 0; d->b_count = 0; d->p_count = 0; d->d_count = 0; }
+  if (tid == 0) {
+    d->bar.count = 0; d->bar.gen = 0; d->dense_sort = 0;
+    d->q_count = 0; d->b_count = 0; d->p_count = 0; d->d_count = 0; d->hot_used = 0;
+    d->ring_pairs[0] = d->ring_pairs[1] = 0; d->ring_warp[0] = d->ring_warp[1] = 0;
+  }
   for (int64_t i = tid; i < p.scan_tiles; i += stride) p.rle_status[i] = 0;
   for (int64_t i = tid; i < p.ids_tiles; i += stride) p.ids_status[i] = 0;
   if (p.single && tid == 0) {
@@ -600,16 +604,17 @@ cudaError_t launch_keys(const Plan& p, cudaStream_t s) {
 // Cooperative launch: every block of the grid must be resident for the grid
 // barriers, so the grid is the occupancy-derived number of resident blocks.
 cudaError_t launch_radix(const Plan& p, cudaStream_t s) {
-  static int blocks_per_sm = 0;
-  if (blocks_per_sm == 0) {
-    cudaError_t e = cudaFuncSetAttribute(k_radix, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)kSweepSmemBytes);
-    if (e != cudaSuccess) return e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_radix, kSortThreads,
-                                                      kSweepSmemBytes);
-    if (e != cudaSuccess) return e;
-    if (blocks_per_sm < 1) return cudaErrorLaunchOutOfResources;
-  }
+  static PerDeviceBlocks cache;
+  int blocks_per_sm = 0;
+  cudaError_t e = cache.get(
+      [](int* b) {
+        cudaError_t r = cudaFuncSetAttribute(k_radix, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)kSweepSmemBytes);
+        if (r != cudaSuccess) return r;
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(b, k_radix, kSortThreads, kSweepSmemBytes);
+      },
+      &blocks_per_sm);
+  if (e != cudaSuccess) return e;
   const int grid = p.num_sms * blocks_per_sm;
   Plan q = p;
   void* args[] = {&q};

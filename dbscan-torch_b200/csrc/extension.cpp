@@ -353,7 +353,8 @@ std::pair<torch::Tensor, std::map<std::string, float>> dbscan2d_profile(torch::T
   return {labels, out};
 }
 
-std::vector<torch::Tensor> dbscan2d_cuda_debug(torch::Tensor X, double eps, int64_t min_samples) {
+std::vector<torch::Tensor> dbscan2d_cuda_debug(torch::Tensor X, double eps, int64_t min_samples,
+                                               bool stable_sort) {
   TORCH_CHECK(X.dim() == 2 && X.size(0) > 0, "debug variant requires n > 0");
   check_input(X, eps, min_samples);
   TORCH_CHECK(X.is_cuda(), "X must be on CUDA");
@@ -388,8 +389,9 @@ std::vector<torch::Tensor> dbscan2d_cuda_debug(torch::Tensor X, double eps, int6
   o.sorted_labels_pre_border = pre.data_ptr<int32_t>();
   o.sorted_labels_final = fin.data_ptr<int32_t>();
   int64_t C = 0;
-  check_rc(dbs_dbscan2d_debug(Xc.data_ptr<float>(), n, eps, min_samples,
-                              labels.data_ptr<int32_t>(), ws.data_ptr(), bytes, stream, &o, &C),
+  check_rc(dbs_dbscan2d_debug_ex(Xc.data_ptr<float>(), n, eps, min_samples,
+                                 labels.data_ptr<int32_t>(), ws.data_ptr(), bytes, stream, &o, &C,
+                                 stable_sort ? DBS_DEBUG_STABLE_SORT : 0),
            "dbscan2d_cuda_debug");
   uint32_t st = 0;
   check_rc(dbs_read_status(ws.data_ptr(), stream, &st), "dbscan2d_cuda_debug");
@@ -517,14 +519,16 @@ std::pair<torch::Tensor, std::map<std::string, int64_t>> dbscan2d_info(torch::Te
   check_rc(dbs_dbscan2d(Xc.data_ptr<float>(), n, eps, min_samples, labels.data_ptr<int32_t>(),
                         ws.data_ptr(), bytes, stream),
            "dbscan2d_info");
-  int64_t cells = 0;
-  int32_t bits = 0, passes = 0, kb = 0;
-  check_rc(dbs_read_plan(ws.data_ptr(), stream, &cells, &bits, &passes, &kb), "dbscan2d_info");
+  dbs_run_stats rs{};
+  check_rc(dbs_read_stats(ws.data_ptr(), stream, &rs), "dbscan2d_info");
   uint32_t st = 0;
   check_rc(dbs_read_status(ws.data_ptr(), stream, &st), "dbscan2d_info");
   raise_if_failed(st);
-  std::map<std::string, int64_t> info{{"num_cells", cells}, {"key_bits", bits},
-                                      {"passes", passes}, {"key_bytes", kb}};
+  std::map<std::string, int64_t> info{
+      {"num_cells", rs.num_cells}, {"key_bits", rs.key_bits}, {"passes", rs.passes},
+      {"key_bytes", rs.key_bytes}, {"hot_slots", rs.hot_slots}, {"queries", rs.queries},
+      {"border", rs.border}, {"pairs_ring0", rs.pairs[0]}, {"pairs_ring1", rs.pairs[1]},
+      {"warp_pairs_ring0", rs.warp_pairs[0]}, {"warp_pairs_ring1", rs.warp_pairs[1]}};
   return {labels, info};
 }
 
@@ -537,8 +541,9 @@ PYBIND11_MODULE(_C, m) {
         pybind11::arg("min_samples"),
         "Profile variant: returns (labels, {stage_name: ms}) with GPU time per reference stage.");
   m.def("dbscan2d_cuda_debug", &dbscan2d_cuda_debug, pybind11::arg("X"), pybind11::arg("eps"),
-        pybind11::arg("min_samples"),
-        "Debug variant: the reference's 11 per-stage intermediate tensors. Not public API.");
+        pybind11::arg("min_samples"), pybind11::arg("stable_sort") = true,
+        "Debug variant: the reference's 11 per-stage intermediate tensors. Not public API. "
+        "stable_sort=False keeps the plain call's sort (points of a cell in arrival order).");
   m.def("dbscan2d_batched", &dbscan2d_batched, pybind11::arg("X"), pybind11::arg("seg_offsets"),
         pybind11::arg("eps"), pybind11::arg("min_samples"),
         "Many clouds in one pipeline run; labels numbered per cloud.");
@@ -553,7 +558,8 @@ PYBIND11_MODULE(_C, m) {
   m.def("workspace_bytes", &workspace_bytes, pybind11::arg("n"), pybind11::arg("nseg") = 1);
   m.def("read_status", &read_status, pybind11::arg("ws"));
   m.def("dbscan2d_info", &dbscan2d_info, pybind11::arg("X"), pybind11::arg("eps"),
-        pybind11::arg("min_samples"), "Labels plus the pipeline's shape (cells, key bits, passes).");
+        pybind11::arg("min_samples"), "Labels plus the pipeline's shape and work counts (cells, key bits, passes, hot-key slots, "
+        "queries, border points, union-find pairs per pass).");
   m.def("check_status", &check_status,
         "Wait for every pending call and raise RuntimeError if one recorded a device failure.");
 }

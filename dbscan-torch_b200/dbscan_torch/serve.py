@@ -89,6 +89,13 @@ class _Lane:
 class DbscanServer:
     """Continuous-batching DBSCAN server on one device (see module docstring).
 
+    Admission: the lanes are sized once from min(budget_bytes, free device
+    memory - RESERVE_BYTES) (``torch.cuda.mem_get_info`` at construction);
+    each lane holds a batch whose footprint (``footprint_bytes`` of its points
+    and clouds) is at most the lane's. Because the lanes are the whole arena,
+    admitting a request into a lane is admitting its footprint against the
+    free-memory budget, without a device allocation per batch.
+
     Args:
         budget_bytes: device memory the arena may use (default 64 GiB).
         lane_points: points per lane; default: the largest that keeps the
@@ -97,13 +104,21 @@ class DbscanServer:
         lanes: number of lanes (concurrent batches).
     """
 
+    RESERVE_BYTES = 1 << 30  # free memory left to the caller
+
     def __init__(self, budget_bytes: int = 64 << 30, lane_points: Optional[int] = None,
                  lane_clouds: int = 1024, lanes: int = 2, device=None):
         self.device = torch.device(device) if device is not None else torch.device(
             "cuda", torch.cuda.current_device())
         if lanes < 1 or lane_clouds < 1:
             raise ValueError("lanes and lane_clouds must be >= 1")
-        per_lane = budget_bytes // lanes
+        # The arena is carved once, from the budget or the free device memory
+        # at construction (less a reserve for the caller's own tensors),
+        # whichever is smaller.
+        free, _ = torch.cuda.mem_get_info(self.device)
+        self.free_bytes_at_start = int(free)
+        usable = min(int(budget_bytes), max(0, int(free) - self.RESERVE_BYTES))
+        per_lane = usable // lanes
         if lane_points is None:
             lo, hi = 1, 64 << 20
             while lo < hi:  # largest lane_points whose footprint fits per_lane
@@ -116,7 +131,7 @@ class DbscanServer:
         if footprint_bytes(lane_points, lane_clouds) > per_lane:
             raise ValueError(f"a lane of {lane_points} points and {lane_clouds} clouds needs "
                              f"{footprint_bytes(lane_points, lane_clouds)} bytes, more than "
-                             f"budget_bytes / lanes = {per_lane}")
+                             f"min(budget_bytes, free device memory - reserve) / lanes = {per_lane}")
         self.budget_bytes = int(budget_bytes)
         self.lane_points = int(lane_points)
         self.lane_clouds = int(lane_clouds)

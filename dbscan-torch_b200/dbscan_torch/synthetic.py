@@ -102,6 +102,19 @@ def batch(n_clouds: int = 4096, seed: int = 0, n_min: int = 256, n_max: int = 26
     return clouds, eps, ms
 
 
+def batch_layout(n_clouds: int = 4096, seed: int = 0, n_min: int = 256, n_max: int = 262_144,
+                 eps_range=(0.2, 1.0), ms_range=(4, 32)):
+    """Sizes, eps and min_samples of the batched workload without the points
+    (for the device generator): sizes log-uniform in [n_min, n_max] (int64),
+    eps_i uniform in eps_range, min_samples_i uniform integers in ms_range
+    (inclusive). Same draws, in the same order, as ``batch``."""
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(np.log(n_min), np.log(n_max), size=n_clouds)).astype(np.int64)
+    eps = rng.uniform(eps_range[0], eps_range[1], size=n_clouds)
+    ms = rng.integers(ms_range[0], ms_range[1] + 1, size=n_clouds)
+    return sizes, eps, ms
+
+
 def request_stream(rate_hz: float = 2000.0, duration_s: float = 60.0, seed: int = 0,
                    n_min: int = 1_000, n_max: int = 2_000_000, eps_range=(0.1, 1.0),
                    ms_range=(4, 32)):

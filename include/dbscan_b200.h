@@ -167,6 +167,44 @@ int dbs_read_status(const void* ws, void* stream, uint32_t* status);
 int dbs_read_plan(const void* ws, void* stream, int64_t* num_cells, int32_t* key_bits,
                   int32_t* passes, int32_t* key_bytes);
 
+/* Work counts of the last call on this workspace, read after synchronising
+ * the stream (no counterpart in the reference, which keeps no counters; the
+ * figures size the work of each stage for profiling and tests):
+ *   num_cells, key_bits, passes, key_bytes  as dbs_read_plan
+ *   hot_slots    occupied slots of the counting sort's 64-slot hot-key table
+ *                (keys that >= 8 lanes of one 32-point row share)
+ *   queries      points of cells below min_samples (counted by distance tests)
+ *   border       non-core points (border assignment candidates)
+ *   pairs[r]     candidate core-cell pairs listed by union pass r (0: side
+ *                neighbours, 1: diagonal and outer ring)
+ *   warp_pairs[r] of those, pairs scanned warp-cooperatively (over budget) */
+typedef struct dbs_run_stats {
+  int64_t num_cells;
+  int32_t key_bits;
+  int32_t passes;
+  int32_t key_bytes;
+  int32_t hot_slots;
+  int64_t queries;
+  int64_t border;
+  int64_t pairs[2];
+  int64_t warp_pairs[2];
+} dbs_run_stats;
+
+int dbs_read_stats(const void* ws, void* stream, dbs_run_stats* out);
+
+/* Debug call with a choice of sort (no counterpart in the reference).
+ * flags = 0: the sort of the plain call -- the counting sort over a dense key
+ * space, which places the points of one cell in arrival order, so perm,
+ * xs, ys, is_core and the sorted labels are permuted within each cell
+ * relative to the reference while keys_sorted, cell_start,
+ * cluster_id_per_cell, uf and every label are the reference's.
+ * flags = DBS_DEBUG_STABLE_SORT: as dbs_dbscan2d_debug (stable radix sort,
+ * every intermediate in the reference's order). */
+#define DBS_DEBUG_STABLE_SORT 1
+int dbs_dbscan2d_debug_ex(const float* X, int64_t n, double eps, int64_t min_samples,
+                          int32_t* labels, void* ws, size_t ws_bytes, void* stream,
+                          const dbs_debug_buffers* out, int64_t* num_cells, int32_t flags);
+
 const char* dbs_strerror(int code);
 const char* dbs_stage_name(int stage);
 

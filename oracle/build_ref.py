@@ -18,7 +18,8 @@ Outputs:
   oracle/_ref/cuda/_C*.so   CPU + CUDA reference (needs libtorch_cuda at import)
   oracle/_ref/cpu/_C*.so    CPU-only reference (fallback when the CUDA build fails)
 
-Usage: python oracle/build_ref.py [--cpu-only] [--src /root/reference]
+Usage: python oracle/build_ref.py --src <reference checkout> [--cpu-only]
+       (or set DBSCAN_REFERENCE_SRC instead of --src)
 """
 
 from __future__ import annotations
@@ -32,7 +33,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
-DEFAULT_SRC = "/root/reference"
+SRC_ENV = "DBSCAN_REFERENCE_SRC"
 
 
 def _build(name: str, sources: list[str], cuda: bool, out_dir: str) -> str:
@@ -70,10 +71,14 @@ def _build(name: str, sources: list[str], cuda: bool, out_dir: str) -> str:
 
 def main(argv: list[str] | None = None) -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--src", default=DEFAULT_SRC)
+    ap.add_argument("--src", default=os.environ.get(SRC_ENV),
+                    help=f"reference checkout (default: ${SRC_ENV})")
     ap.add_argument("--cpu-only", action="store_true")
     ap.add_argument("--one", choices=["cpu", "cuda"], help=argparse.SUPPRESS)
     args = ap.parse_args(argv)
+    if not args.src:
+        print(f"no reference checkout given (--src or ${SRC_ENV}); nothing built")
+        return 0
     csrc = os.path.join(args.src, "csrc")
     if not os.path.isdir(csrc):
         print(f"reference sources not found at {csrc}; nothing built")

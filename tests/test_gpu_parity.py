@@ -44,6 +44,50 @@ def test_debug_intermediates_match_oracle(name, X, eps, ms):
         assert np.array_equal(a, b), f"{name}/{k}: {(a != b).sum()} entries differ"
 
 
+def _to_input_order(perm, sorted_vals):
+    out = np.empty_like(sorted_vals)
+    out[perm] = sorted_vals
+    return out
+
+
+@pytest.mark.parametrize("name,X,eps,ms", CASES, ids=IDS)
+def test_counting_sort_intermediates(name, X, eps, ms):
+    """The plain call's counting sort (dense key spaces) places the points of
+    a cell in arrival order, not the reference's stable order. Every
+    order-free intermediate must still equal the oracle's: the sorted keys,
+    the cells, cluster id per cell, union-find roots and every label; the
+    points of each cell are the same set; per-point values (sorted
+    coordinates, core flags, sorted labels) equal the oracle's once mapped to
+    input order through perm."""
+    Xd = torch.from_numpy(X).cuda()
+    _, info = _C.dbscan2d_info(Xd, eps, ms)
+    if info["passes"] != 0:
+        pytest.skip("sparse key space: the plain call takes the radix sort")
+    out = _C.dbscan2d_cuda_debug(Xd, eps, ms, stable_sort=False)
+    names = ["labels", "keys_sorted", "perm", "xs", "ys", "is_core", "cell_start",
+             "cluster_id_per_cell", "uf", "sorted_labels_pre_border", "sorted_labels_final"]
+    d = {k: t.cpu().numpy() for k, t in zip(names, out)}
+    o = oracle.dbscan2d(X, eps, ms, debug=True)
+    for k in ("labels", "cell_start", "cluster_id_per_cell", "uf"):
+        assert np.array_equal(d[k], o[k]), f"{name}/{k}: {(d[k] != o[k]).sum()} entries differ"
+    assert np.array_equal(d["keys_sorted"], o["keys_sorted"].view(np.int64)), f"{name}/keys_sorted"
+    n = X.shape[0]
+    perm = d["perm"]
+    assert np.array_equal(np.sort(perm), np.arange(n)), f"{name}: perm is not a permutation"
+    cs = d["cell_start"]
+    cell_of = np.repeat(np.arange(cs.size - 1), np.diff(cs))
+    mine = perm[np.lexsort((perm, cell_of))]
+    theirs = o["perm"][np.lexsort((o["perm"], cell_of))]
+    assert np.array_equal(mine, theirs), f"{name}: cells hold different points"
+    xs, ys = d["xs"], d["ys"]
+    assert np.array_equal(xs.view(np.uint32), X[perm, 0].view(np.uint32)), f"{name}/xs"
+    assert np.array_equal(ys.view(np.uint32), X[perm, 1].view(np.uint32)), f"{name}/ys"
+    for k in ("is_core", "sorted_labels_pre_border", "sorted_labels_final"):
+        a = _to_input_order(perm, d[k])
+        b = _to_input_order(o["perm"], o[k])
+        assert np.array_equal(a, b), f"{name}/{k}: {(a != b).sum()} points differ"
+
+
 def test_repeated_runs_bit_identical():
     for make in (datasets.dense_overlapping_blobs, datasets.near_percolation_uniform):
         X = torch.from_numpy(make(50_000, 0)).cuda()

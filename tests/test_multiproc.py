@@ -35,7 +35,8 @@ def _worker(rank, world, port, q):
     try:
         import bench
         from dbscan_torch.shard import shard_clouds, shard_loads
-        sizes, _, _ = bench.batch_config(4096)
+        from dbscan_torch.synthetic import batch_layout
+        sizes, _, _ = batch_layout(4096, seed=0)
         shards = shard_clouds(sizes, world)
         gathered = [None] * world
         dist.all_gather_object(gathered, shards[rank])
@@ -58,9 +59,8 @@ def test_two_gloo_ranks():
         p.join(timeout=60)
         assert p.exitcode == 0
     results.sort()
-    sys.path.insert(0, ROOT)
-    import bench
-    sizes, _, _ = bench.batch_config(4096)
+    from dbscan_torch.synthetic import batch_layout
+    sizes, _, _ = batch_layout(4096, seed=0)
     for rank, gathered, shards, m, loads in results:
         assert m == 3.0                      # max over ranks of 1.5, 3.0
         assert gathered == shards            # every rank computed the same assignment

@@ -1,13 +1,24 @@
-"""Serving loop (dbscan_torch.serve): every request's labels equal a plain
-dbscan2d call on that cloud alone; admission respects the lane capacity and
-the device-memory budget; queued requests are batched."""
+"""Serving loop (dbscan_torch.serve): every request's labels equal the
+oracle's labels for that cloud (bit-exact) and a plain dbscan2d call on that
+cloud alone -- the same result alone and in the mix; admission respects the
+lane capacity and the device-memory budget; queued requests are batched."""
 
 import numpy as np
 import pytest
 import torch
 
+import oracle
 from dbscan_torch import DbscanServer, dbscan2d, footprint_bytes, synthetic
 from dbscan_torch import _C
+
+
+def _check(r):
+    """Request r's labels against the oracle and against a plain call alone."""
+    want = oracle.dbscan2d(r.X.numpy(), r.eps, r.min_samples)
+    got = r.labels.numpy()
+    assert np.array_equal(got, want), f"request {r.rid} (n={r.n}): {(got != want).sum()} labels differ from the oracle"
+    alone = dbscan2d(r.X.cuda(), r.eps, r.min_samples).cpu()
+    assert torch.equal(r.labels, alone), f"request {r.rid} (n={r.n}): differs from the plain call"
 
 
 def test_footprint_monotone():
@@ -36,8 +47,7 @@ def test_serve_matches_plain():
     assert srv.completed == len(reqs) and srv.batches < len(reqs)
     for r in reqs:
         assert r.done and r.latency >= 0
-        want = dbscan2d(r.X.cuda(), r.eps, r.min_samples).cpu()
-        assert torch.equal(r.labels, want), f"request {r.rid} (n={r.n})"
+        _check(r)
 
 
 @pytest.mark.gpu
@@ -51,7 +61,7 @@ def test_serve_interleaved_submit():
         srv.step()
     srv.drain()
     for r in reqs:
-        assert torch.equal(r.labels, dbscan2d(r.X.cuda(), r.eps, r.min_samples).cpu())
+        _check(r)
 
 
 @pytest.mark.gpu
@@ -69,5 +79,5 @@ def test_serve_admission():
     reqs = [srv.submit(X, 0.5, 10) for _ in range(12)]
     srv.drain()
     assert srv.batches >= 4
-    want = dbscan2d(X.cuda(), 0.5, 10).cpu()
+    want = torch.from_numpy(oracle.dbscan2d(X.numpy(), 0.5, 10))
     assert all(torch.equal(r.labels, want) for r in reqs)

@@ -155,5 +155,21 @@ def test_hot_keys(order):
         ms = 4
     ours, info = _C.dbscan2d_info(torch.from_numpy(X).cuda(), EPS, ms)
     assert info["passes"] == 0, info  # the counting sort ran
+    if order == "cell_order":
+        # Nearly every row is hot: all 64 slots are taken and later hot keys
+        # find their probe window full and stay cold.
+        assert info["hot_slots"] == 64, info
+    else:
+        # The dominant cell's key (and few others) went through the table.
+        assert 1 <= info["hot_slots"] < 64, info
     want = oracle.dbscan2d(X, EPS, ms)
     assert np.array_equal(ours.cpu().numpy(), want)
+
+
+def test_spread_keys_stay_cold():
+    """A shuffled constant-density cloud has no row with 8 points of one cell:
+    the hot-key table stays empty, every point takes the cold path."""
+    X = synthetic.constant_density(300_000, seed=8)
+    ours, info = _C.dbscan2d_info(torch.from_numpy(X).cuda(), EPS, 10)
+    assert info["passes"] == 0 and info["hot_slots"] == 0, info
+    assert np.array_equal(ours.cpu().numpy(), oracle.dbscan2d(X, EPS, 10))
