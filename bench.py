@@ -67,19 +67,22 @@ WORKLOAD = "constant_density_10M"
 DATA = "synthetic (seeded constant-density Gaussian blobs + 2% noise)"
 L2_FLUSH_BYTES = 512 << 20
 # Kernel launches of one dbscan2d call (tests/test_launch_count.py counts them
-# with the profiler): init, bounds, seg_finalize | csort_clear, csort_count,
-# csort, keys, radix | rle | cell_prep, huge_bbox | core, status |
-# 2 x (pairs, pair_scan, pair_warp) + flatten | ids, cid | labels. Kernels
-# whose work the device-side plan skips (radix passes under the counting
-# sort, the huge-cell pass without huge cells) still launch and return at once.
-KERNELS_PER_CALL = 23
+# with the profiler): init, bounds, seg_finalize | bkt_part, bkt_local,
+# csort_clear, csort_count, csort, keys, radix | rle | cell_prep, huge_bbox |
+# core, status | 2 x (pairs, pair_scan, pair_warp) + flatten | ids, cid |
+# labels. Kernels whose work the device-side plan skips (the sort forms that
+# do not run, the huge-cell pass without huge cells) still launch and return
+# at once.
+KERNELS_PER_CALL = 25
 # Launches per reference stage (the profile entry point times stages).
-STAGE_LAUNCHES = {"cell_keys": 3, "sort_gather": 5, "boundary_scan": 1, "build_ngh": 2,
+STAGE_LAUNCHES = {"cell_keys": 3, "sort_gather": 7, "boundary_scan": 1, "build_ngh": 2,
                   "core_mark": 2, "union_find": 7, "cluster_id": 2, "border_assign": 1}
 # The kernels that do a stage's work on this workload (the others of the
-# stage return at once).
-STAGE_KERNEL = {"sort_gather": ("k_csort_clear", "k_csort_count", "k_csort"),
-                "build_ngh": ("k_cell_prep",), "core_mark": ("k_core",),
+# stage return at once); the sort's depend on the form that ran.
+SORT_KERNELS = {0: ("k_keys", "k_radix"), 1: ("k_csort_clear", "k_csort_count", "k_csort"),
+                2: ("k_bkt_part", "k_bkt_local")}
+SORT_FORM_NAME = {0: "radix", 1: "counting", 2: "bucketed counting"}
+STAGE_KERNEL = {"build_ngh": ("k_cell_prep",), "core_mark": ("k_core",),
                 "border_assign": ("k_labels",)}
 PROFILE_MD = os.path.join(ROOT, "profiles", "kernels_constant_density_10M.md")
 
@@ -460,7 +463,9 @@ def run_ours(args, world, rank, local):
     cells, passes, kb = info["num_cells"], info["passes"], info["key_bytes"]
     sb = stage_bytes(N_POINTS, cells, passes, kb)
     dom = max(STAGE_LAUNCHES, key=lambda s: prof[s])
-    kernels = STAGE_KERNEL.get(dom, (dom,)) if (dom != "sort_gather" or passes == 0) else ("k_keys", "k_radix")
+    form = info["sort_form"]
+    stage_kernels = dict(STAGE_KERNEL, sort_gather=SORT_KERNELS[form])
+    kernels = stage_kernels.get(dom, (dom,))
     kernel = "+".join(kernels)
     peak, peak_kind = _peaks()
     # The stage's kernels (one launch each) do its work; the stage time also
@@ -471,7 +476,7 @@ def run_ours(args, world, rank, local):
             "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "peak_source": peak_kind,
             "alg_bytes_per_launch": sb[dom],
-            "traffic": ncu_traffic(kernels) if dom in STAGE_KERNEL else None,
+            "traffic": ncu_traffic(kernels) if dom in stage_kernels else None,
             "pipeline_alg_bytes": b_alg_total,
             "pipeline_frac": round(b_alg_total / (ms_mean * 1e-3) / 1e9 / peak, 4),
             "stage_ms": {s: round(v, 4) for s, v in prof.items()},
@@ -502,8 +507,9 @@ def run_ours(args, world, rank, local):
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
            "data": DATA, "config": base_config(world),
            "pipeline": {"num_cells": cells, "key_bits": info["key_bits"], "radix_passes": passes,
-                        "sort": "counting" if passes == 0 else "radix",
-                        "queries": info["queries"], "border_points": info["border"],
+                        "sort": SORT_FORM_NAME[form], "buckets": info["buckets"],
+                        "queries": info["queries"], "query_cells": info["query_cells"],
+                        "border_points": info["border"], "border_cells": info["border_cells"],
                         "union_pairs": [info["pairs_ring0"], info["pairs_ring1"]],
                         "union_warp_pairs": [info["warp_pairs_ring0"], info["warp_pairs_ring1"]]},
            "clocks": clocks.summary(),
@@ -597,6 +603,7 @@ def run_batched(dev, n_clouds: int) -> dict:
     plan = pkg.BatchedPlan(offl)
     plan.run(X, eps, ms)  # captures the graph (built-in shape)
     t_plan = statistics.median([_ev_ms(plan.run)[0] for _ in range(3)])
+    gaps = graph_gaps(plan, t_plan)
     t0 = time.perf_counter()
     tuned = plan.tune()
     tune_s = time.perf_counter() - t0
@@ -621,7 +628,25 @@ def run_batched(dev, n_clouds: int) -> dict:
                                              tuned["shape"])),
                      "builtin_shape": list(tuned["default_shape"]),
                      "tune_s": round(tune_s, 2), "shapes_timed": tuned["trials"],
-                     "labels_equal": bool(equal_tuned)}}
+                     "labels_equal": bool(equal_tuned), "launch_gaps": gaps}}
+
+
+def graph_gaps(plan, graph_ms: float) -> dict:
+    """Launch gaps inside one replay of the plan's graph: the kernels' own
+    durations (a CUPTI trace of one replay through torch.profiler) against
+    the replay's CUDA-event time measured without the profiler. The
+    difference bounds what one persistent launch of the whole pipeline could
+    save."""
+    torch.cuda.synchronize()
+    with torch.profiler.profile(activities=[torch.profiler.ProfilerActivity.CUDA]) as prof:
+        plan.run()
+        torch.cuda.synchronize()
+    kern = [e for e in prof.events() if e.device_type == torch.autograd.DeviceType.CUDA
+            and ("k_" in e.name or "dbs::" in e.name)]
+    ksum = sum(e.device_time_total for e in kern) / 1e3  # us -> ms
+    return {"kernels": len(kern), "kernel_sum_ms": round(ksum, 3), "graph_ms": round(graph_ms, 3),
+            "gap_ms": round(graph_ms - ksum, 3),
+            "gap_per_launch_us": round((graph_ms - ksum) * 1e3 / max(1, len(kern)), 2)}
 
 
 def run_configs(dev) -> dict:

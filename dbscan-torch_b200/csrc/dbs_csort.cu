@@ -40,31 +40,6 @@ namespace dbs {
 constexpr int kCsThreads = 256;
 constexpr uint32_t kFullMask = 0xffffffffu;
 
-// Per-cloud scalars of the dense key of a point (its dense-map index, which
-// fits 31 bits), held in registers while a thread's points stay in one cloud.
-struct KeyCtx {
-  int32_t bx[4], by[4];
-  uint64_t px, py, base;
-  uint32_t ysh;
-  float inv_r;
-  int64_t end;  // first input index past the cloud
-  int32_t seg;
-  __device__ void load(const Plan& p, int32_t s) {
-    const SegInfo& g = p.seg_info[s];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) { bx[k] = g.bx[k]; by[k] = g.by[k]; }
-    px = g.px; py = g.py; base = g.base; ysh = g.ysh;
-    inv_r = p.seg_param[s].inv_r;
-    end = p.seg_off[s + 1];
-    seg = s;
-  }
-  __device__ uint32_t key(float2 v) const {
-    const uint64_t gx = compact_axis(cell_coord(v.x, inv_r), bx, px);
-    const uint64_t gy = compact_axis(cell_coord(v.y, inv_r), by, py);
-    return (uint32_t)(base + (gx << ysh) + gy);
-  }
-};
-
 // Points per lane and iteration of the point loops: independent loads and
 // atomics in flight per thread.
 constexpr int kU = 4;
@@ -136,18 +111,6 @@ __device__ __forceinline__ int hot_find(const Plan& p, uint32_t key) {
     if (k == kHotEmpty) return -1;
   }
   return -1;
-}
-
-// Cloud owning global key b: the last cloud whose key base is <= b (empty
-// clouds share their base with the next cloud and come before it).
-__device__ __forceinline__ int32_t seg_of_key(const Plan& p, uint64_t b) {
-  if (p.nseg == 1) return 0;
-  int32_t lo = 0, hi = p.nseg - 1;
-  while (lo < hi) {
-    const int32_t mid = (lo + hi + 1) >> 1;
-    if (p.seg_info[mid].base <= b) lo = mid; else hi = mid - 1;
-  }
-  return lo;
 }
 
 // Block-wide exclusive scan of two counters; returns the block totals.
@@ -380,7 +343,7 @@ __global__ void __launch_bounds__(kCsThreads, 6) k_csort_count(Plan p) {
 __global__ void __launch_bounds__(kCsThreads, 5) k_csort(Plan p) {
   __shared__ uint32_t s_a[kCsThreads / 32], s_b[kCsThreads / 32];
   Desc* d = p.desc;
-  if (!d->dense_sort) return;
+  if (d->dense_sort != 1u) return;  // radix sort, or the bucketed sort ran
   const int64_t n = p.n;
   const int64_t W = (int64_t)d->dense_total;
   uint32_t* bins = p.bin_count;

@@ -67,6 +67,22 @@ constexpr int kHotSlots = 64;
 constexpr uint32_t kHotGroup = 8;
 constexpr int64_t kDenseSlack = 4096;
 
+// Bucketed counting sort (dbs_bsort.cu), for dense key spaces of runs with
+// at least kBktMinPoints points: the key space is cut into at most
+// kBktMaxBuckets buckets of 2^bkt_shift <= kBktMaxKeys consecutive keys; a
+// partition pass moves every point into its bucket's run, a local pass
+// counting-sorts each bucket in shared memory. A bucket holding more than
+// kBktCap points (a few huge cells) sends the run to the global counting
+// sort instead, whose hot-key path handles them.
+constexpr int kBktMaxBuckets = 4096;
+constexpr int kBktMaxKeys = 8192;
+constexpr int kBktMaxChunks = 1024;     // blocks of the cooperative partition
+constexpr int64_t kBktMinPoints = 1 << 18;
+constexpr uint32_t kBktCap = 1u << 16;
+constexpr int kBktTile = 4096;          // points per partition tile
+constexpr int kBktThreads = 256;
+constexpr int kBktTargetBuckets = 2048;  // buckets aimed at (fewer keys per bucket)
+
 // Grid-stride kernels whose grid (blocks per SM) a launch shape may set
 // (dbs_launch_shape of the C-ABI, same indices), and their built-in grids.
 // The label pass takes 32 blocks per SM while its border items go first
@@ -113,6 +129,7 @@ enum : int {
   kCtrLabels,
   kCtrBig,
   kCtrDebug,
+  kCtrBkt,
   kNumCtr
 };
 
@@ -161,12 +178,18 @@ struct Desc {
   unsigned long long big_packed;  // huge cells: entries << 40 | chunks
   uint32_t ctr[kNumCtr];
   uint32_t digit_total[2][kRadix];  // per-pass digit totals (ping-pong)
-  uint32_t dense_sort;  // 1: counting sort over the dense key space
-  uint32_t q_count;     // core-query list length (points of cells below ms)
-  uint32_t b_count;     // border list length (non-core points)
+  uint32_t dense_sort;  // 1: counting sort over the dense key space, 2: bucketed counting sort
+  uint32_t q_count;     // query-cell list length (cells below min_samples)
+  uint32_t b_count;     // border-cell list length (cells holding a non-core point)
   uint32_t p_count;     // union-find candidate pair list length
   uint32_t d_count;     // pairs deferred to warp-cooperative scans
   uint32_t hot_used;    // counting sort: occupied hot-key slots
+  uint32_t qp_count;    // points of the query cells
+  uint32_t bp_count;    // non-core points
+  uint32_t bkt_ok;      // bucketed sort possible (dense, enough points, buckets fit)
+  uint32_t bkt_shift;   // log2 keys per bucket
+  uint32_t bkt_nb;      // buckets
+  uint32_t bkt_max;     // points in the largest bucket
   uint32_t ring_pairs[2];  // p_count of each union pass (kept for the stats read-back)
   uint32_t ring_warp[2];   // d_count of each union pass
   GridBar bar;
@@ -202,8 +225,8 @@ struct Plan {
   int32_t* uf;            // (n)
   int32_t* root_rank;     // (n) exclusive scan of root flags
   int32_t* cid;           // (n) cluster id per cell
-  uint32_t* qlist;        // (n) sorted positions needing a core count
-  uint32_t* blist;        // (n) sorted positions of non-core points
+  uint32_t* qlist;        // (n) query cells: cells below min_samples (core counts needed)
+  uint32_t* blist;        // (n) border cells: cells holding a non-core point
   int2* plist;            // (pair_cap) candidate cell pairs (c, nc > c)
   uint32_t* dlist;        // (pair_cap) indices into plist, over budget
   int64_t pair_cap;       // entries available in plist / dlist
@@ -222,6 +245,11 @@ struct Plan {
   uint32_t* hot_cnt;      //   points of hot rows per hot key
   uint32_t* hot_cold;     //   points of the key outside hot rows
   uint32_t* hot_base;     //   first sorted position of the key's hot points
+  uint32_t* bkt_mat;      // bucketed sort: per-(bucket, chunk) counts -> offsets, bucket-major
+                          //   (nullptr when n < kBktMinPoints: path disabled)
+  uint32_t* bkt_tot;      //   points per bucket (kBktMaxBuckets)
+  uint32_t* bkt_start;    //   first record of each bucket (kBktMaxBuckets + 1)
+  unsigned long long* bkt_status;  // look-back words of the local pass (kBktMaxBuckets)
   int32_t force_radix;    // debug entry: stable radix sort (reference perm)
   int64_t n;
   int32_t nseg;
@@ -312,6 +340,56 @@ __device__ __forceinline__ int32_t expand_axis(uint64_t g, const int32_t b[4], u
   if (g < pw) return (int32_t)((uint32_t)b[0] + (uint32_t)g);
   return (int32_t)((uint32_t)b[2] + (uint32_t)(g - pw));
 }
+
+// Cloud owning global key b: the last cloud whose key base is <= b (empty
+// clouds share their base with the next cloud and come before it).
+__device__ __forceinline__ int32_t seg_of_key(const Plan& p, uint64_t b) {
+  if (p.nseg == 1) return 0;
+  int32_t lo = 0, hi = p.nseg - 1;
+  while (lo < hi) {
+    const int32_t mid = (lo + hi + 1) >> 1;
+    if (p.seg_info[mid].base <= b) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Bucket width of a dense key space of W keys: the fewest keys per bucket
+// (a power of two) that keeps the buckets at or below kBktTargetBuckets,
+// widened up to kBktMaxKeys; ~0 when even then more than kBktMaxBuckets
+// buckets would be needed.
+__device__ __forceinline__ uint32_t bkt_shift_for(uint64_t W, uint32_t* nb) {
+  uint32_t sh = 0;
+  while (sh < 13 && ((W + (1ull << sh) - 1) >> sh) > (uint64_t)kBktTargetBuckets) ++sh;
+  const uint64_t buckets = (W + (1ull << sh) - 1) >> sh;
+  if ((1u << sh) > (uint32_t)kBktMaxKeys || buckets > (uint64_t)kBktMaxBuckets || buckets == 0) return ~0u;
+  *nb = (uint32_t)buckets;
+  return sh;
+}
+
+// Per-cloud scalars of the dense key of a point (its dense-map index, which
+// fits 31 bits), held in registers while a thread's points stay in one cloud.
+struct KeyCtx {
+  int32_t bx[4], by[4];
+  uint64_t px, py, base;
+  uint32_t ysh;
+  float inv_r;
+  int64_t end;  // first input index past the cloud
+  int32_t seg;
+  __device__ void load(const Plan& p, int32_t s) {
+    const SegInfo& g = p.seg_info[s];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) { bx[k] = g.bx[k]; by[k] = g.by[k]; }
+    px = g.px; py = g.py; base = g.base; ysh = g.ysh;
+    inv_r = p.seg_param[s].inv_r;
+    end = p.seg_off[s + 1];
+    seg = s;
+  }
+  __device__ uint32_t key(float2 v) const {
+    const uint64_t gx = compact_axis(cell_coord(v.x, inv_r), bx, px);
+    const uint64_t gy = compact_axis(cell_coord(v.y, inv_r), by, py);
+    return (uint32_t)(base + (gx << ysh) + gy);
+  }
+};
 
 __device__ __forceinline__ void set_error(Desc* d, uint32_t bits) {
   atomicOr(&d->status, bits);
@@ -445,6 +523,7 @@ cudaError_t launch_front(const Plan& p, cudaStream_t s);      // init, bounds, f
 cudaError_t launch_keys(const Plan& p, cudaStream_t s);
 cudaError_t launch_radix(const Plan& p, cudaStream_t s);
 cudaError_t launch_csort(const Plan& p, cudaStream_t s);
+cudaError_t launch_bsort(const Plan& p, cudaStream_t s);
 cudaError_t launch_rle(const Plan& p, cudaStream_t s);
 cudaError_t launch_cell_prep(const Plan& p, cudaStream_t s);
 cudaError_t launch_core(const Plan& p, cudaStream_t s);

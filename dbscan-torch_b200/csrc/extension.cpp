@@ -503,6 +503,24 @@ int64_t read_status(torch::Tensor ws) {
 
 void check_status() { drain(true); }
 
+// Work counts of the last run on a workspace (dbs_read_stats), synchronising.
+std::map<std::string, int64_t> stats_dict(const void* ws, cudaStream_t stream) {
+  dbs_run_stats rs{};
+  check_rc(dbs_read_stats(ws, stream, &rs), "read_stats");
+  return {{"num_cells", rs.num_cells}, {"key_bits", rs.key_bits}, {"passes", rs.passes},
+          {"key_bytes", rs.key_bytes}, {"hot_slots", rs.hot_slots}, {"sort_form", rs.sort_form},
+          {"buckets", rs.buckets}, {"queries", rs.queries}, {"query_cells", rs.query_cells},
+          {"border", rs.border}, {"border_cells", rs.border_cells},
+          {"pairs_ring0", rs.pairs[0]}, {"pairs_ring1", rs.pairs[1]},
+          {"warp_pairs_ring0", rs.warp_pairs[0]}, {"warp_pairs_ring1", rs.warp_pairs[1]}};
+}
+
+std::map<std::string, int64_t> read_stats(torch::Tensor ws) {
+  TORCH_CHECK(ws.is_cuda(), "ws must be on CUDA");
+  c10::cuda::CUDAGuard guard(ws.device());
+  return stats_dict(ws.data_ptr(), at::cuda::getCurrentCUDAStream());
+}
+
 // Plain call that also reports the pipeline's shape (synchronises): labels,
 // {num_cells, key_bits, passes, key_bytes}.
 std::pair<torch::Tensor, std::map<std::string, int64_t>> dbscan2d_info(torch::Tensor X, double eps,
@@ -519,17 +537,10 @@ std::pair<torch::Tensor, std::map<std::string, int64_t>> dbscan2d_info(torch::Te
   check_rc(dbs_dbscan2d(Xc.data_ptr<float>(), n, eps, min_samples, labels.data_ptr<int32_t>(),
                         ws.data_ptr(), bytes, stream),
            "dbscan2d_info");
-  dbs_run_stats rs{};
-  check_rc(dbs_read_stats(ws.data_ptr(), stream, &rs), "dbscan2d_info");
   uint32_t st = 0;
   check_rc(dbs_read_status(ws.data_ptr(), stream, &st), "dbscan2d_info");
   raise_if_failed(st);
-  std::map<std::string, int64_t> info{
-      {"num_cells", rs.num_cells}, {"key_bits", rs.key_bits}, {"passes", rs.passes},
-      {"key_bytes", rs.key_bytes}, {"hot_slots", rs.hot_slots}, {"queries", rs.queries},
-      {"border", rs.border}, {"pairs_ring0", rs.pairs[0]}, {"pairs_ring1", rs.pairs[1]},
-      {"warp_pairs_ring0", rs.warp_pairs[0]}, {"warp_pairs_ring1", rs.warp_pairs[1]}};
-  return {labels, info};
+  return {labels, stats_dict(ws.data_ptr(), stream)};
 }
 
 PYBIND11_MODULE(_C, m) {
@@ -557,6 +568,8 @@ PYBIND11_MODULE(_C, m) {
   m.def("fill_seg_params", &fill_seg_params, pybind11::arg("eps"), pybind11::arg("min_samples"));
   m.def("workspace_bytes", &workspace_bytes, pybind11::arg("n"), pybind11::arg("nseg") = 1);
   m.def("read_status", &read_status, pybind11::arg("ws"));
+  m.def("read_stats", &read_stats, pybind11::arg("ws"),
+        "Work counts of the last run on a workspace (cells, sort form, buckets, queries, pairs).");
   m.def("dbscan2d_info", &dbscan2d_info, pybind11::arg("X"), pybind11::arg("eps"),
         pybind11::arg("min_samples"), "Labels plus the pipeline's shape and work counts (cells, key bits, passes, hot-key slots, "
         "queries, border points, union-find pairs per pass).");

@@ -136,6 +136,11 @@ class BatchedPlan:
         self.graph.replay()
         return self.labels
 
+    def stats(self) -> dict:
+        """Work counts of the last run (cells, sort form, buckets, core
+        queries, border points, union-find pairs); synchronises."""
+        return dict(_C.read_stats(self.ws))
+
     def status(self) -> int:
         """Device status word of the last run (0 = ok); synchronises."""
         return int(_C.read_status(self.ws))

@@ -13,7 +13,7 @@ import torch
 import datasets
 import oracle
 import refmod
-from dbscan_torch import _C, dbscan2d, dbscan2d_batched
+from dbscan_torch import _C, dbscan2d, dbscan2d_batched, synthetic
 
 pytestmark = pytest.mark.gpu
 
@@ -63,6 +63,21 @@ def test_counting_sort_intermediates(name, X, eps, ms):
     _, info = _C.dbscan2d_info(Xd, eps, ms)
     if info["passes"] != 0:
         pytest.skip("sparse key space: the plain call takes the radix sort")
+    _check_unstable_intermediates(name, X, Xd, eps, ms)
+
+
+@pytest.mark.parametrize("n,ms", [(1_000_000, 10), (400_000, 3)])
+def test_bucketed_sort_intermediates(n, ms):
+    """Clouds of 2^18 points or more take the bucketed counting sort: the same
+    order-free intermediates as the oracle's."""
+    X = synthetic.constant_density(n, seed=4) if n >= 10**6 else datasets.dense_overlapping_blobs(n, 3)
+    Xd = torch.from_numpy(X).cuda()
+    _, info = _C.dbscan2d_info(Xd, 0.5, ms)
+    assert info["sort_form"] == 2, info
+    _check_unstable_intermediates(f"bucketed_{n}", X, Xd, 0.5, ms)
+
+
+def _check_unstable_intermediates(name, X, Xd, eps, ms):
     out = _C.dbscan2d_cuda_debug(Xd, eps, ms, stable_sort=False)
     names = ["labels", "keys_sorted", "perm", "xs", "ys", "is_core", "cell_start",
              "cluster_id_per_cell", "uf", "sorted_labels_pre_border", "sorted_labels_final"]
