@@ -508,8 +508,7 @@ def run_ours(args, world, rank, local):
            "data": DATA, "config": base_config(world),
            "pipeline": {"num_cells": cells, "key_bits": info["key_bits"], "radix_passes": passes,
                         "sort": SORT_FORM_NAME[form], "buckets": info["buckets"],
-                        "queries": info["queries"], "query_cells": info["query_cells"],
-                        "border_points": info["border"], "border_cells": info["border_cells"],
+                        "queries": info["queries"], "border_points": info["border"],
                         "union_pairs": [info["pairs_ring0"], info["pairs_ring1"]],
                         "union_warp_pairs": [info["warp_pairs_ring0"], info["warp_pairs_ring1"]]},
            "clocks": clocks.summary(),
@@ -839,10 +838,15 @@ def main():
                     help="length of the config-4 serving stream (0 skips serving)")
     ap.add_argument("--serve-sweep-seconds", type=float, default=3.0,
                     help="length of each offered-rate step of the saturation sweep")
+    ap.add_argument("--points", type=int, default=N_POINTS,
+                    help="points of the main constant-density workload (smaller clouds for "
+                         "profiler captures; the benchmark line is the 10M-point cloud)")
     ap.add_argument("--leg", choices=["cpu", "ref_cuda"], help=argparse.SUPPRESS)
     ap.add_argument("--points-file", help=argparse.SUPPRESS)
     ap.add_argument("--labels-out", help=argparse.SUPPRESS)
     args = ap.parse_args()
+    if args.points != N_POINTS:
+        globals().update(N_POINTS=int(args.points), WORKLOAD=f"constant_density_{int(args.points)}")
     if args.leg:
         print(json.dumps(run_leg(args)), flush=True)
         return

@@ -50,6 +50,7 @@ namespace {
 constexpr uint32_t kFull = 0xffffffffu;
 constexpr int kBktWarps = kBktThreads / 32;
 constexpr int kPartItems = kBktTile / kBktThreads;  // points per thread per tile
+constexpr int kLocalItems = 8;                      // records per thread per step of the local pass
 
 // Dynamic shared memory of k_bkt_part.
 struct PartSmem {
@@ -124,15 +125,28 @@ __global__ void __launch_bounds__(kBktThreads, 2) k_bkt_part(Plan p) {
   uint32_t* const rec_key = reinterpret_cast<uint32_t*>(p.keys[1]);
   mark_phase(d, 0);
 
-  // 1. histogram of this chunk's buckets
+  // 1. histogram of this chunk's buckets (kPartItems independent loads in
+  //    flight per thread, as in the partition)
   for (int b = threadIdx.x; b < NB; b += blockDim.x) sm.cnt[b] = 0;
   __syncthreads();
   if (c0 < c1) {
     KeyCtx kc;
     kc.load(p, seg_of(p, c0 + min((int64_t)threadIdx.x, c1 - c0 - 1)));
-    for (int64_t i = c0 + threadIdx.x; i < c1; i += blockDim.x) {
-      while (i >= kc.end) kc.load(p, kc.seg + 1);
-      atomicAdd(&sm.cnt[kc.key(p.X[i]) >> shift], 1u);
+    for (int64_t tile = c0; tile < c1; tile += kBktTile) {
+      float2 v[kPartItems];
+#pragma unroll
+      for (int k = 0; k < kPartItems; ++k) {
+        const int64_t i = tile + k * kBktThreads + threadIdx.x;
+        v[k] = i < c1 ? p.X[i] : make_float2(0.f, 0.f);
+      }
+#pragma unroll
+      for (int k = 0; k < kPartItems; ++k) {
+        const int64_t i = tile + k * kBktThreads + threadIdx.x;
+        if (i < c1) {
+          while (i >= kc.end) kc.load(p, kc.seg + 1);
+          atomicAdd(&sm.cnt[kc.key(v[k]) >> shift], 1u);
+        }
+      }
     }
   }
   __syncthreads();
@@ -268,10 +282,19 @@ __global__ void __launch_bounds__(kBktThreads) k_bkt_local(Plan p) {
     for (int k = threadIdx.x; k < kn; k += blockDim.x) s_cnt[k] = 0;
     __syncthreads();
 
-    // 5. key counts
-    for (uint32_t r = rs + threadIdx.x; r < re; r += blockDim.x) {
-      const uint32_t key = one ? kc0.key(rec_xy[r]) : rec_key[r];
-      atomicAdd(&s_cnt[key - (uint32_t)kb0], 1u);
+    // 5. key counts (kLocalItems independent loads in flight per thread)
+    for (uint32_t r0 = rs; r0 < re; r0 += kLocalItems * kBktThreads) {
+      uint32_t key[kLocalItems];
+#pragma unroll
+      for (int k = 0; k < kLocalItems; ++k) {
+        const uint32_t r = r0 + k * kBktThreads + threadIdx.x;
+        if (r < re) key[k] = one ? kc0.key(rec_xy[r]) : rec_key[r];
+      }
+#pragma unroll
+      for (int k = 0; k < kLocalItems; ++k) {
+        const uint32_t r = r0 + k * kBktThreads + threadIdx.x;
+        if (r < re) atomicAdd(&s_cnt[key[k] - (uint32_t)kb0], 1u);
+      }
     }
     __syncthreads();
 
@@ -347,16 +370,32 @@ __global__ void __launch_bounds__(kBktThreads) k_bkt_local(Plan p) {
     }
     __syncthreads();
 
-    // 7. place the records
-    for (uint32_t r = rs + threadIdx.x; r < re; r += blockDim.x) {
-      const float2 v = rec_xy[r];
-      const uint32_t key = one ? kc0.key(v) : rec_key[r];
-      const uint32_t at = rs + atomicAdd(&s_cnt[key - (uint32_t)kb0], 1u);
-      if (at < re) {
-        p.perm[at] = rec_idx[r];
-        p.xy[at] = v;
-      } else {
-        set_error(d, kErrCapacity);
+    // 7. place the records (loads batched as in step 5)
+    for (uint32_t r0 = rs; r0 < re; r0 += kLocalItems * kBktThreads) {
+      float2 v[kLocalItems];
+      uint32_t key[kLocalItems], idx[kLocalItems];
+#pragma unroll
+      for (int k = 0; k < kLocalItems; ++k) {
+        const uint32_t r = r0 + k * kBktThreads + threadIdx.x;
+        if (r < re) {
+          v[k] = rec_xy[r];
+          idx[k] = rec_idx[r];
+          if (!one) key[k] = rec_key[r];
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < kLocalItems; ++k) {
+        const uint32_t r = r0 + k * kBktThreads + threadIdx.x;
+        if (r < re) {
+          const uint32_t kk = one ? kc0.key(v[k]) : key[k];
+          const uint32_t at = rs + atomicAdd(&s_cnt[kk - (uint32_t)kb0], 1u);
+          if (at < re) {
+            p.perm[at] = idx[k];
+            p.xy[at] = v[k];
+          } else {
+            set_error(d, kErrCapacity);
+          }
+        }
       }
     }
     __syncthreads();
@@ -387,7 +426,7 @@ cudaError_t launch_bsort(const Plan& p, cudaStream_t s) {
   e = cudaLaunchCooperativeKernel((const void*)k_bkt_part, dim3(grid), dim3(kBktThreads), args,
                                   kPartSmemBytes, s);
   if (e != cudaSuccess) return e;
-  k_bkt_local<<<p.num_sms * 4, kBktThreads, 0, s>>>(p);
+  k_bkt_local<<<p.num_sms * 8, kBktThreads, 0, s>>>(p);
   return cudaGetLastError();
 }
 

@@ -508,10 +508,8 @@ int dbs_read_stats(const void* ws, void* stream, dbs_run_stats* out) {
   out->hot_slots = (int32_t)h.hot_used;
   out->sort_form = (int32_t)h.dense_sort;
   out->buckets = h.dense_sort == 2u ? (int32_t)h.bkt_nb : 0;
-  out->queries = h.qp_count;
-  out->query_cells = h.q_count;
-  out->border = h.bp_count;
-  out->border_cells = h.b_count;
+  out->queries = h.q_count;
+  out->border = h.b_count;
   // The flatten between the passes saved pass 0's counts; pass 1's are the
   // live counters.
   out->pairs[0] = h.ring_pairs[0];

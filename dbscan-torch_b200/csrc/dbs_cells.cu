@@ -16,7 +16,7 @@
 // cell's points and resolves the 25 offsets of the 5x5 stencil in the
 // reference's order (off = (dx+2)*5 + (dy+2)); the warp then walks its cells'
 // contiguous points to record each point's cell and class (core wholesale,
-// k_core_pass1 :199-208) and lists the cells below min_samples for k_core.
+// or a query for k_core; k_core_pass1 :199-208).
 #include "dbs_internal.cuh"
 
 namespace dbs {
@@ -165,9 +165,9 @@ __device__ __forceinline__ void append_list(uint32_t* list, uint32_t* count, boo
 //     theirs from the whole warp; cells above kHugeCell from k_huge_bbox);
 //   - the warp's cells own one contiguous range of sorted points: each point
 //     gets its cell, and its class (k_core_pass1, dbscan_cuda.cu:199-208): a
-//     point of a cell with >= ms points is core wholesale. Point-parallel, so
-//     the stores are coalesced. Cells below ms go to the query-cell list of
-//     k_core;
+//     point of a cell with >= ms points is core wholesale, any other point
+//     goes to the query list of k_core. Point-parallel, so the stores are
+//     coalesced;
 //   - the 25-entry neighbour row of each cell, staged in shared memory and
 //     written as one contiguous block per warp.
 __global__ void __launch_bounds__(kCellThreads, 5) k_cell_prep(Plan p) {
@@ -264,14 +264,9 @@ __global__ void __launch_bounds__(kCellThreads, 5) k_cell_prep(Plan p) {
           p.point_cell[i] = (int32_t)(wbase + lo);
           p.is_core[i] = dn ? 1 : 0;
         }
+        append_list(p.qlist, &p.desc->q_count, ok && !dn, (uint32_t)i);
       }
     }
-    // Query cells (below ms, huge ones included): k_core counts their points'
-    // neighbours, one warp per cell.
-    const bool query = valid && !dense;
-    append_list(p.qlist, &p.desc->q_count, query, c);
-    const uint32_t qpts = __reduce_add_sync(full, query ? (uint32_t)(s1 - s0) : 0u);
-    if (lane == 0 && qpts) atomicAdd(&p.desc->qp_count, qpts);
 
     // Neighbour row, off = (dx+2)*5 + (dy+2) as in the reference.
     if (valid) {
@@ -349,8 +344,7 @@ __global__ void __launch_bounds__(256) k_huge_bbox(Plan p) {
     const int32_t a = s0 + k * kHugeChunk, b = min(s1, a + kHugeChunk);
     float xmin = INFINITY, xmax = -INFINITY, ymin = INFINITY, ymax = -INFINITY;
     // The chunk's points also get their cell and class, as k_cell_prep gives
-    // every other point (a huge cell is below ms only when ms > kHugeCell;
-    // k_cell_prep lists such a cell for k_core).
+    // every other point (a huge cell is below ms only when ms > kHugeCell).
     const bool dn = (s1 - s0) >= p.seg_param[p.cell_seg[c]].ms;
     for (int32_t base = a; base < b; base += 32) {
       const int32_t i = base + (int32_t)lane;
@@ -365,6 +359,7 @@ __global__ void __launch_bounds__(256) k_huge_bbox(Plan p) {
         xmin = fminf(xmin, v.x); xmax = fmaxf(xmax, v.x);
         ymin = fminf(ymin, v.y); ymax = fmaxf(ymax, v.y);
       }
+      append_list(p.qlist, &d->q_count, ok && !dn, (uint32_t)i);
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {

@@ -7,15 +7,14 @@
 //   thrust::exclusive_scan :698-701, k_cluster_id_per_cell :392-404,
 //   k_core_labels :409-417, k_border_assign :427-470, k_unpermute :475-481.
 //
-// Core marking runs one warp per query cell (a cell below min_samples,
-// listed by k_cell_prep): the cell's neighbour rows, boxes and point ranges
-// are read once, and the pair tests of all its queries are packed over the
-// lanes. Union-find works on compacted cell-pair lists: one thread per
-// candidate pair, one warp per pair over the thread's test budget. Border
-// assignment runs one warp per cell holding a non-core point, packed the same
-// way; core labels one warp per 256 sorted points. The reference's
-// bounding-box prunes are kept exactly, so every pair the reference tests is
-// tested with the same arithmetic and the same verdict.
+// Core marking runs one thread per query point (the points of cells below
+// min_samples, listed by k_cell_prep in sorted order, so a warp's threads are
+// mostly points of one cell and share its neighbour row, boxes and candidate
+// points). Union-find works on compacted cell-pair lists: one thread per
+// candidate pair, one warp per pair over the thread's test budget. Labelling
+// runs one thread per border point, then one per sorted point. The
+// reference's bounding-box prunes are kept exactly, so every pair the
+// reference tests is tested with the same arithmetic and the same verdict.
 #include "dbs_internal.cuh"
 
 namespace dbs {
@@ -41,141 +40,75 @@ __device__ __forceinline__ void append(uint32_t* list, uint32_t* count, bool tak
 __constant__ int8_t kNearFirst[24] = {7, 11, 13, 17, 6, 8, 16, 18, 2, 10, 14, 22,
                                       1, 3, 5, 9, 15, 19, 21, 23, 0, 4, 20, 24};
 
-// Pair tests of one neighbour cell against the open queries of a warp.
-// The queries (lanes with `need`) are compacted into ord[0, na); the
-// neighbour's points j0 .. j1 are taken in chunks of M = min(|nb|, 32), and
-// each pass of the warp covers qpi = 32 / M queries at once: lane l tests
-// candidate j0 + l % M against query ord[g + l / M]. A 15-point neighbour
-// thus keeps 30 of 32 lanes busy, and its points are read once per chunk
-// with one coalesced load (`load(cj, valid)`, into registers).
-// `visit(ok, cand, qx, qy, src, mine, my_mask)` runs on every lane of every
-// pass: ok = the lane holds a real (query, candidate) pair, src = the lane of
-// its query, mine = this lane's own query is in this pass, and my_mask = the
-// lanes that test this lane's query.
-template <typename Load, typename Visit>
-__device__ __forceinline__ void scan_pairs(float2 q, bool need, int32_t j0, int32_t j1, uint8_t* ord,
-                                           Load load, Visit visit) {
-  const uint32_t lane = lane_id();
-  const uint32_t act = __ballot_sync(kFull, need);
-  const int na = __popc(act);
-  const int rank = __popc(act & lanemask_lt());
-  if (need) ord[rank] = (uint8_t)lane;
-  __syncwarp();
-  const int nbs = j1 - j0;
-  const int M = nbs < 32 ? nbs : 32;
-  const int qpi = 32 / M;
-  const int slot = (int)lane / M, cl = (int)lane - slot * M;
-  const int my_s = rank % qpi, my_g = rank - my_s;
-  const uint32_t my_mask = (M == 32 ? kFull : ((1u << M) - 1u)) << (my_s * M);
-  for (int32_t jb = j0; jb < j1; jb += 32) {
-    const int32_t cj = jb + cl;
-    const bool cv = slot < qpi && cj < j1;
-    const auto cand = load(cj, cv);
-    for (int g = 0; g < na; g += qpi) {
-      const int qs = g + slot;
-      const bool ok = cv && qs < na;
-      const int src = ord[ok ? qs : 0];
-      const float qx = __shfl_sync(kFull, q.x, src), qy = __shfl_sync(kFull, q.y, src);
-      visit(ok, cand, qx, qy, src, need && g == my_g, my_mask);
-    }
-  }
-  __syncwarp();  // ord is rewritten by the next neighbour
-}
-
-// Core flags of the points of the query cells (cells with fewer than
-// min_samples points; k_core_pass2, dbscan_cuda.cu:213-245), one warp per
-// cell. Lane k holds the k-th nearest stencil cell of the query cell (row
-// entry, box, point range), so the 24 neighbour rows are read once per cell
-// instead of once per query point. Each query counts its own cell wholesale
-// (the reference never distance-tests the centre cell, :231-233), then walks
-// the neighbours nearest first: a neighbour that fails the query's point-box
-// prune (:235) is skipped, one wholly within eps of the query
-// (point_box_max_d2, the same rounded form) counts all its points, and the
-// rest are tested pairwise (scan_pairs); a query stops once its count
-// reaches min_samples. None of these change the core flag. Queries that stay
-// non-core are border candidates, found again by k_status through the cell.
+// Core flag of every query point, one thread per query. A query counts its
+// own cell wholesale (the reference never distance-tests the centre cell,
+// :231-233) plus the points within eps of the other 24 stencil cells that
+// survive the point-box prune (:235-240), stopping once the count reaches
+// ms (k_core_pass2 :213-245). Queries that stay non-core go to the border
+// list of k_labels.
 __global__ void __launch_bounds__(kCellThreads) k_core(Plan p) {
-  __shared__ uint8_t s_ord[kCellThreads / 32][32];
-  const uint32_t lane = lane_id();
-  uint8_t* ord = s_ord[threadIdx.x >> 5];
-  const uint32_t nq = p.desc->q_count;
-  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < nq; w += nwarps) {
-    const int32_t c = (int32_t)p.qlist[w];
-    const int32_t s0 = p.cell_start[c], s1 = p.cell_start[c + 1];
-    const SegParam sp = p.seg_param[p.cell_seg[c]];
-    const float eps_sq = sp.eps_sq;
-    int32_t nb_l = -1, j0_l = 0, j1_l = 0;
-    float4 bb_l = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (lane < kNgh - 1) {
-      nb_l = p.ngh[(int64_t)c * kNgh + kNearFirst[lane]];
-      if (nb_l >= 0) {
-        bb_l = p.bbox[nb_l];
-        j0_l = p.cell_start[nb_l];
-        j1_l = p.cell_start[nb_l + 1];
-      }
-    }
-    for (int32_t qb = s0; qb < s1; qb += 32) {
-      const int32_t qi = qb + (int32_t)lane;
-      const bool qv = qi < s1;
-      const float2 q = qv ? p.xy[qi] : make_float2(0.f, 0.f);
-      int32_t cnt = s1 - s0;
-      bool open = qv && cnt < sp.ms;
-      for (int k = 0; k < kNgh - 1; ++k) {
-        if (__ballot_sync(kFull, open) == 0) break;
-        const int32_t nb = __shfl_sync(kFull, nb_l, k);
+  const uint32_t qn = p.desc->q_count;
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t base = blockIdx.x * blockDim.x; base < qn; base += stride) {
+    const uint32_t t = base + threadIdx.x;
+    bool noncore = false;
+    uint32_t i = 0;
+    if (t < qn) {
+      i = p.qlist[t];
+      const int32_t c = p.point_cell[i];
+      const int32_t st0 = p.cell_start[c], st1 = p.cell_start[c + 1];
+      const SegParam sp = p.seg_param[p.cell_seg[c]];
+      const int32_t ms = sp.ms;
+      const float eps_sq = sp.eps_sq;
+      int32_t cnt = st1 - st0;
+      const float2 q = p.xy[i];
+      const int32_t* row = p.ngh + (int64_t)c * kNgh;
+      // Nearest cells first, so the count reaches ms (and stops) sooner; a
+      // neighbour cell wholly within eps of q (point_box_max_d2) counts all
+      // its points without distance tests. Neither changes the core flag.
+      for (int o = 0; o < kNgh - 1 && cnt < ms; ++o) {
+        const int32_t nb = row[kNearFirst[o]];
         if (nb < 0) continue;
-        const float4 bb = make_float4(__shfl_sync(kFull, bb_l.x, k), __shfl_sync(kFull, bb_l.y, k),
-                                      __shfl_sync(kFull, bb_l.z, k), __shfl_sync(kFull, bb_l.w, k));
-        const int32_t j0 = __shfl_sync(kFull, j0_l, k), j1 = __shfl_sync(kFull, j1_l, k);
-        bool need = open && point_box_d2(q.x, q.y, bb) <= eps_sq;
-        if (need && point_box_max_d2(q.x, q.y, bb) <= eps_sq) {
+        const float4 bb = p.bbox[nb];
+        if (!(point_box_d2(q.x, q.y, bb) <= eps_sq)) continue;
+        const int32_t j0 = p.cell_start[nb], j1 = p.cell_start[nb + 1];
+        if (point_box_max_d2(q.x, q.y, bb) <= eps_sq) {
           cnt += j1 - j0;
-          need = false;
+          continue;
         }
-        if (__ballot_sync(kFull, need) != 0) {
-          scan_pairs(q, need, j0, j1, ord,
-                     [&](int32_t cj, bool cv) { return cv ? p.xy[cj] : make_float2(0.f, 0.f); },
-                     [&](bool ok, float2 pj, float qx, float qy, int, bool mine, uint32_t my_mask) {
-                       const bool hit = ok && sq_dist(__fsub_rn(pj.x, qx), __fsub_rn(pj.y, qy)) <= eps_sq;
-                       const uint32_t hb = __ballot_sync(kFull, hit);
-                       if (mine) cnt += __popc(hb & my_mask);
-                     });
+        for (int32_t j = j0; j < j1; ++j) {
+          const float2 pj = p.xy[j];
+          cnt += sq_dist(__fsub_rn(pj.x, q.x), __fsub_rn(pj.y, q.y)) <= eps_sq;
         }
-        open = open && cnt < sp.ms;
       }
-      if (qv) p.is_core[qi] = cnt >= sp.ms ? 1 : 0;
+      const bool core = cnt >= ms;
+      p.is_core[i] = core ? 1 : 0;
+      noncore = !core;
     }
+    append(p.blist, &p.desc->b_count, noncore, i);
   }
 }
 
 // Cell status (dbscan_cuda.cu:250-263) and union-find initialisation
-// (:313-316), one thread per cell; cells holding a non-core point go to the
-// border-cell list of k_labels.
+// (:313-316), one thread per cell.
 __global__ void __launch_bounds__(256) k_status(Plan p) {
-  Desc* d = p.desc;
-  const uint32_t C = d->num_cells;
-  const uint32_t stride = gridDim.x * blockDim.x;
-  for (uint32_t base = blockIdx.x * blockDim.x; base < C; base += stride) {
-    const uint32_t c = base + threadIdx.x;
-    uint32_t noncore = 0;
-    if (c < C) {
-      const int32_t s0 = p.cell_start[c], s1 = p.cell_start[c + 1];
-      uint8_t st;
-      if (s1 - s0 >= p.seg_param[p.cell_seg[c]].ms) {
-        st = 2;
-      } else {
-        uint32_t nc = 0;
-        for (int32_t j = s0; j < s1; ++j) nc += p.is_core[j] == 0;
-        noncore = nc;
-        st = nc == (uint32_t)(s1 - s0) ? 0 : (nc == 0 ? 2 : 1);
+  const uint32_t C = p.desc->num_cells;
+  for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < C; c += gridDim.x * blockDim.x) {
+    const int32_t s0 = p.cell_start[c], s1 = p.cell_start[c + 1];
+    uint8_t st;
+    if (s1 - s0 >= p.seg_param[p.cell_seg[c]].ms) {
+      st = 2;
+    } else {
+      bool any = false, all = true;
+      for (int32_t j = s0; j < s1; ++j) {
+        const bool k = p.is_core[j] != 0;
+        any |= k;
+        all &= k;
       }
-      p.cell_status[c] = st;
-      p.uf[c] = (int32_t)c;
+      st = !any ? 0 : (all ? 2 : 1);
     }
-    append(p.blist, &d->b_count, noncore != 0, c);
-    const uint32_t tot = __reduce_add_sync(kFull, noncore);
-    if (lane_id() == 0 && tot) atomicAdd(&d->bp_count, tot);
+    p.cell_status[c] = st;
+    p.uf[c] = (int32_t)c;
   }
 }
 
@@ -537,121 +470,66 @@ __global__ void __launch_bounds__(256) k_cid(Plan p) {
 
 // --------------------------------------------------------------- k_labels
 // Final labels, written straight to input order (k_core_labels :409-417,
-// k_border_assign :427-470, k_unpermute :475-481). Work items, taken by
-// warps from a counter: one per border cell (a cell holding a non-core
-// point), then one per 256 sorted points for the core labels (each core
-// point takes its cell's id). With labels that fit L2 (n <= kCoreFirstPoints)
-// the border cells go first, so their uneven scans overlap the core items of
-// other warps; with more points the core items go first, so the whole grid
-// sweeps the sorted points -- and the input-order label writes of the clouds
-// there -- together instead of scattering them over the whole label array.
-//
-// A border cell's warp holds the centre cell and the 24 other stencil cells
-// (nearest first) one per lane, skipping cells without a core point. Each
-// non-core point of the cell takes the cluster of the core point within eps
-// that minimises (d2, input index) -- the reference's tie rule -- or -1. A
-// neighbour whose box is farther than the best d2 found so far is skipped
-// (point_box_d2 is a lower bound of its points' rounded d2, so none can win;
-// a box at exactly the best d2 is still scanned for a tie with a smaller
-// index). Pair tests are packed over the lanes as in k_core, and each
-// query's minimum key lives in shared memory (atomicMin on u64).
-constexpr int32_t kLabelChunk = 256;  // sorted points per core-label item
-
-struct CorePt {
-  float2 xy;
-  uint32_t idx;  // input index (perm), ~0 for a non-core point
-};
-
-__device__ __forceinline__ void border_cell(const Plan& p, int32_t c, uint8_t* ord,
-                                            unsigned long long* s_best) {
-  const uint32_t lane = lane_id();
-  const int32_t s0 = p.cell_start[c], s1 = p.cell_start[c + 1];
-  const float eps_sq = p.seg_param[p.cell_seg[c]].eps_sq;
-  int32_t nb_l = -1, j0_l = 0, j1_l = 0;
-  float4 bb_l = make_float4(0.f, 0.f, 0.f, 0.f);
-  if (lane < kNgh) {
-    nb_l = p.ngh[(int64_t)c * kNgh + (lane == 0 ? 12 : kNearFirst[lane - 1])];
-    if (nb_l >= 0 && p.cell_status[nb_l] == 0) nb_l = -1;
-    if (nb_l >= 0) {
-      bb_l = p.bbox[nb_l];
-      j0_l = p.cell_start[nb_l];
-      j1_l = p.cell_start[nb_l + 1];
-    }
-  }
-  for (int32_t qb = s0; qb < s1; qb += 32) {
-    const int32_t qi = qb + (int32_t)lane;
-    const bool qv = qi < s1 && !p.is_core[qi];
-    if (__ballot_sync(kFull, qv) == 0) continue;
-    const float2 q = qv ? p.xy[qi] : make_float2(0.f, 0.f);
-    unsigned long long best = ~0ull;
-    int32_t best_nb = -1;
-    float best_d2 = eps_sq;  // no candidate beyond this (eps, then the best so far)
-    s_best[lane] = ~0ull;
-    __syncwarp();
-    for (int k = 0; k < kNgh; ++k) {
-      const int32_t nb = __shfl_sync(kFull, nb_l, k);
-      if (nb < 0) continue;
-      const float4 bb = make_float4(__shfl_sync(kFull, bb_l.x, k), __shfl_sync(kFull, bb_l.y, k),
-                                    __shfl_sync(kFull, bb_l.z, k), __shfl_sync(kFull, bb_l.w, k));
-      const int32_t j0 = __shfl_sync(kFull, j0_l, k), j1 = __shfl_sync(kFull, j1_l, k);
-      const bool need = qv && point_box_d2(q.x, q.y, bb) <= best_d2;
-      if (__ballot_sync(kFull, need) == 0) continue;
-      // Candidates: core points only (others carry idx = ~0 and never win).
-      scan_pairs(q, need, j0, j1, ord,
-                 [&](int32_t cj, bool cv) {
-                   CorePt cp{make_float2(0.f, 0.f), ~0u};
-                   if (cv && p.is_core[cj]) { cp.xy = p.xy[cj]; cp.idx = p.perm[cj]; }
-                   return cp;
-                 },
-                 [&](bool ok, const CorePt& cp, float qx, float qy, int src, bool, uint32_t) {
-                   if (ok && cp.idx != ~0u) {
-                     const float d2 = sq_dist(__fsub_rn(cp.xy.x, qx), __fsub_rn(cp.xy.y, qy));
-                     // d2 >= +0 and not NaN here, so its bits order like its value.
-                     if (d2 <= eps_sq)
-                       atomicMin(&s_best[src], ((unsigned long long)__float_as_uint(d2) << 32) | cp.idx);
-                   }
-                 });
-      if (need) {
-        const unsigned long long b = s_best[lane];
-        if (b < best) {
-          best = b;
-          best_nb = nb;
-          best_d2 = __uint_as_float((uint32_t)(b >> 32));
-        }
-      }
-    }
-    if (qv) p.labels[p.perm[qi]] = best_nb < 0 ? -1 : p.cid[best_nb];
-    __syncwarp();  // s_best is reset for the next group
-  }
-}
+// k_border_assign :427-470, k_unpermute :475-481). Items [0, b_count) are
+// the non-core points of the border list: each takes the cluster of the
+// core point within eps that minimises (d2, input index) over the 25
+// stencil cells with a core point, pruned by the point-box test, or -1.
+// Items after that are all sorted points; core ones take their cell's id.
+// Item order: with labels that fit L2 (n <= kCoreFirstPoints, 64 MB), the
+// border items go first so their uneven scans overlap the core items of
+// other warps (121 us against 136 us at 10M points); with more points the
+// core items go first, so the whole grid sweeps the sorted points -- and the
+// input-order label writes of the clouds there -- together instead of
+// scattering them over the whole label array (3.5 ms against 7.6 ms for a
+// 151M-point, 4,096-cloud batch).
 
 __global__ void __launch_bounds__(kCellThreads) k_labels(Plan p) {
-  __shared__ uint8_t s_ord[kCellThreads / 32][32];
-  __shared__ unsigned long long s_best[kCellThreads / 32][32];
-  const uint32_t lane = lane_id();
-  const int wib = threadIdx.x >> 5;
   const int64_t n = p.n;
-  const int64_t nbc = p.desc->b_count;
-  const int64_t nchunks = (n + kLabelChunk - 1) / kLabelChunk;
-  const int64_t total = nbc + nchunks;
+  const int64_t bn = p.desc->b_count;
+  const int64_t total = bn + n;
   const bool core_first = n > kCoreFirstPoints;
-  while (true) {
-    uint32_t w = 0;
-    if (lane == 0) w = atomicAdd(&p.desc->ctr[kCtrLabels], 1u);
-    w = __shfl_sync(kFull, w, 0);
-    if ((int64_t)w >= total) break;
-    const int64_t bt = core_first ? (int64_t)w - nchunks : (int64_t)w;  // border-cell item
-    if (bt >= 0 && bt < nbc) {
-      border_cell(p, (int32_t)p.blist[bt], s_ord[wib], s_best[wib]);
-      continue;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t i;
+    int32_t lab;
+    const int64_t bt = core_first ? t - n : t;  // index into the border list
+    if (bt >= 0 && bt < bn) {
+      i = p.blist[bt];
+      const int32_t c = p.point_cell[i];
+      const float eps_sq = p.seg_param[p.cell_seg[c]].eps_sq;
+      const float2 q = p.xy[i];
+      const int32_t* row = p.ngh + (int64_t)c * kNgh;
+      unsigned long long best = ~0ull;
+      int32_t best_nb = -1;
+      float best_d2 = eps_sq;  // no candidate beyond this (eps, then the best so far)
+      // Centre cell, then nearest cells first. A cell whose box is farther
+      // than the best d2 found so far cannot hold a smaller (d2, index) key:
+      // its points are all strictly farther (point_box_d2 is a lower bound of
+      // their rounded d2). A box at exactly the best d2 is still scanned, for
+      // a tie with a smaller index.
+      for (int o = -1; o < kNgh - 1; ++o) {
+        const int32_t nb = row[o < 0 ? 12 : kNearFirst[o]];
+        if (nb < 0 || p.cell_status[nb] == 0) continue;
+        if (!(point_box_d2(q.x, q.y, p.bbox[nb]) <= best_d2)) continue;
+        const int32_t j1 = p.cell_start[nb + 1];
+        for (int32_t j = p.cell_start[nb]; j < j1; ++j) {
+          if (!p.is_core[j]) continue;
+          const float2 pj = p.xy[j];
+          const float d2 = sq_dist(__fsub_rn(pj.x, q.x), __fsub_rn(pj.y, q.y));
+          if (d2 <= eps_sq) {
+            // d2 >= +0 and not NaN here, so its bits order like its value.
+            const unsigned long long key = ((unsigned long long)__float_as_uint(d2) << 32) | p.perm[j];
+            if (key < best) { best = key; best_nb = nb; best_d2 = d2; }
+          }
+        }
+      }
+      lab = best_nb < 0 ? -1 : p.cid[best_nb];
+    } else {
+      i = core_first ? t : t - bn;
+      if (!p.is_core[i]) continue;
+      lab = p.cid[p.point_cell[i]];
     }
-    const int64_t chunk = core_first ? (int64_t)w : (int64_t)w - nbc;
-    const int64_t i0 = chunk * kLabelChunk;
-#pragma unroll 4
-    for (int k = 0; k < kLabelChunk / 32; ++k) {
-      const int64_t i = i0 + k * 32 + lane;
-      if (i < n && p.is_core[i]) p.labels[p.perm[i]] = p.cid[p.point_cell[i]];
-    }
+    p.labels[p.perm[i]] = lab;
   }
 }
 

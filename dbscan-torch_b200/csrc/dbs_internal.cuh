@@ -75,7 +75,7 @@ constexpr int64_t kDenseSlack = 4096;
 // kBktCap points (a few huge cells) sends the run to the global counting
 // sort instead, whose hot-key path handles them.
 constexpr int kBktMaxBuckets = 4096;
-constexpr int kBktMaxKeys = 8192;
+constexpr int kBktMaxKeys = 4096;
 constexpr int kBktMaxChunks = 1024;     // blocks of the cooperative partition
 constexpr int64_t kBktMinPoints = 1 << 18;
 constexpr uint32_t kBktCap = 1u << 16;
@@ -179,13 +179,11 @@ struct Desc {
   uint32_t ctr[kNumCtr];
   uint32_t digit_total[2][kRadix];  // per-pass digit totals (ping-pong)
   uint32_t dense_sort;  // 1: counting sort over the dense key space, 2: bucketed counting sort
-  uint32_t q_count;     // query-cell list length (cells below min_samples)
-  uint32_t b_count;     // border-cell list length (cells holding a non-core point)
+  uint32_t q_count;     // core-query list length (points of cells below ms)
+  uint32_t b_count;     // border list length (non-core points)
   uint32_t p_count;     // union-find candidate pair list length
   uint32_t d_count;     // pairs deferred to warp-cooperative scans
   uint32_t hot_used;    // counting sort: occupied hot-key slots
-  uint32_t qp_count;    // points of the query cells
-  uint32_t bp_count;    // non-core points
   uint32_t bkt_ok;      // bucketed sort possible (dense, enough points, buckets fit)
   uint32_t bkt_shift;   // log2 keys per bucket
   uint32_t bkt_nb;      // buckets
@@ -225,8 +223,8 @@ struct Plan {
   int32_t* uf;            // (n)
   int32_t* root_rank;     // (n) exclusive scan of root flags
   int32_t* cid;           // (n) cluster id per cell
-  uint32_t* qlist;        // (n) query cells: cells below min_samples (core counts needed)
-  uint32_t* blist;        // (n) border cells: cells holding a non-core point
+  uint32_t* qlist;        // (n) sorted positions needing a core count
+  uint32_t* blist;        // (n) sorted positions of non-core points
   int2* plist;            // (pair_cap) candidate cell pairs (c, nc > c)
   uint32_t* dlist;        // (pair_cap) indices into plist, over budget
   int64_t pair_cap;       // entries available in plist / dlist
@@ -359,7 +357,7 @@ __device__ __forceinline__ int32_t seg_of_key(const Plan& p, uint64_t b) {
 // buckets would be needed.
 __device__ __forceinline__ uint32_t bkt_shift_for(uint64_t W, uint32_t* nb) {
   uint32_t sh = 0;
-  while (sh < 13 && ((W + (1ull << sh) - 1) >> sh) > (uint64_t)kBktTargetBuckets) ++sh;
+  while ((1u << sh) < (uint32_t)kBktMaxKeys && ((W + (1ull << sh) - 1) >> sh) > (uint64_t)kBktTargetBuckets) ++sh;
   const uint64_t buckets = (W + (1ull << sh) - 1) >> sh;
   if ((1u << sh) > (uint32_t)kBktMaxKeys || buckets > (uint64_t)kBktMaxBuckets || buckets == 0) return ~0u;
   *nb = (uint32_t)buckets;

@@ -44,7 +44,7 @@ __global__ void k_init(Plan p) {
   if (tid == 0) {
     d->bar.count = 0; d->bar.gen = 0; d->dense_sort = 0;
     d->q_count = 0; d->b_count = 0; d->p_count = 0; d->d_count = 0; d->hot_used = 0;
-    d->qp_count = 0; d->bp_count = 0; d->bkt_ok = 0; d->bkt_max = 0;
+    d->bkt_ok = 0; d->bkt_max = 0;
     d->ring_pairs[0] = d->ring_pairs[1] = 0; d->ring_warp[0] = d->ring_warp[1] = 0;
   }
   for (int64_t i = tid; i < p.scan_tiles; i += stride) p.rle_status[i] = 0;

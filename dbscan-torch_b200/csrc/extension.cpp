@@ -509,8 +509,7 @@ std::map<std::string, int64_t> stats_dict(const void* ws, cudaStream_t stream) {
   check_rc(dbs_read_stats(ws, stream, &rs), "read_stats");
   return {{"num_cells", rs.num_cells}, {"key_bits", rs.key_bits}, {"passes", rs.passes},
           {"key_bytes", rs.key_bytes}, {"hot_slots", rs.hot_slots}, {"sort_form", rs.sort_form},
-          {"buckets", rs.buckets}, {"queries", rs.queries}, {"query_cells", rs.query_cells},
-          {"border", rs.border}, {"border_cells", rs.border_cells},
+          {"buckets", rs.buckets}, {"queries", rs.queries}, {"border", rs.border},
           {"pairs_ring0", rs.pairs[0]}, {"pairs_ring1", rs.pairs[1]},
           {"warp_pairs_ring0", rs.warp_pairs[0]}, {"warp_pairs_ring1", rs.warp_pairs[1]}};
 }

@@ -20,9 +20,10 @@ Structure:
   lane is free and requests are queued, launches every queued request that
   fits (first come, first served) as one batched pipeline run: one
   host-to-device copy per request into the lane's point buffer, one copy of
-  the cloud tables, the segmented pipeline, one device-to-host copy of all
-  labels and of the device status word. Completion is observed through CUDA
-  events, never by blocking the host.
+  the cloud tables, the segmented pipeline, one device-to-host copy per
+  request straight into that request's own pinned label tensor, and one of
+  the device status word. Completion is observed through CUDA events, never
+  by blocking the host.
 
 Host inputs should be pinned (``torch.Tensor.pin_memory()``) for the copies
 to be asynchronous.
@@ -49,8 +50,9 @@ def footprint_bytes(n: int, nseg: int = 1) -> int:
 
 @dataclass
 class Request:
-    """One clustering request. ``labels`` (a CPU int32 tensor) is set when
-    ``done``; ``t_submit`` / ``t_done`` are ``time.perf_counter()`` stamps."""
+    """One clustering request. ``labels`` (a pinned CPU int32 tensor) holds
+    the result once ``done``; ``t_submit`` / ``t_done`` are
+    ``time.perf_counter()`` stamps."""
     X: torch.Tensor
     eps: float
     min_samples: int
@@ -77,7 +79,6 @@ class _Lane:
     offsets: torch.Tensor
     params: torch.Tensor
     ws: torch.Tensor
-    labels_host: torch.Tensor
     offsets_host: torch.Tensor
     params_host: torch.Tensor
     status_host: torch.Tensor
@@ -146,7 +147,6 @@ class DbscanServer:
                 offsets=torch.zeros(S + 1, dtype=torch.int64, device=d),
                 params=torch.zeros(S * 16, dtype=torch.uint8, device=d),
                 ws=torch.empty(int(_C.workspace_bytes(P, S)), dtype=torch.uint8, device=d),
-                labels_host=torch.empty(P, dtype=torch.int32).pin_memory(),
                 offsets_host=torch.zeros(S + 1, dtype=torch.int64).pin_memory(),
                 params_host=torch.zeros(S * 16, dtype=torch.uint8).pin_memory(),
                 status_host=torch.zeros(4, dtype=torch.uint8).pin_memory(),
@@ -210,6 +210,8 @@ class DbscanServer:
         off = np.zeros(S + 1, dtype=np.int64)
         np.cumsum(sizes, out=off[1:])
         lane.offsets_host[: S + 1].copy_(torch.from_numpy(off))
+        for r in batch:
+            r.labels = torch.empty(r.n, dtype=torch.int32, pin_memory=True)
         eps = torch.tensor([r.eps for r in batch], dtype=torch.float64)
         ms = torch.tensor([r.min_samples for r in batch], dtype=torch.int64)
         lane.params_host[: S * 16].copy_(_C.fill_seg_params(eps, ms))
@@ -224,7 +226,11 @@ class DbscanServer:
             if total:
                 _C.dbscan2d_batched_into(lane.X[:total], lane.offsets[: S + 1], lane.params[: S * 16],
                                          lane.labels[:total], lane.ws)
-                lane.labels_host[:total].copy_(lane.labels[:total], non_blocking=True)
+                # Each request's labels go straight into its own pinned tensor
+                # (caching host allocator): no host-side copy when it retires.
+                for k, r in enumerate(batch):
+                    if r.n:
+                        r.labels.copy_(lane.labels[off[k]: off[k + 1]], non_blocking=True)
                 lane.status_host.copy_(lane.ws[:4], non_blocking=True)
             lane.event.record(lane.stream)
         lane.batch = batch
@@ -237,10 +243,7 @@ class DbscanServer:
             raise RuntimeError(f"dbscan2d (serving): device-side failure (status 0x{st:x}) in a batch of "
                                f"{len(lane.batch)} requests; their labels are invalid")
         now = time.perf_counter()
-        pos = 0
         for r in lane.batch:
-            r.labels = lane.labels_host[pos: pos + r.n].clone()
-            pos += r.n
             r.t_done = now
             r.done = True
         n = len(lane.batch)

@@ -180,9 +180,7 @@ int dbs_read_plan(const void* ws, void* stream, int64_t* num_cells, int32_t* key
  *   warp_pairs[r] of those, pairs scanned warp-cooperatively (over budget)
  *   sort_form    0 radix sort, 1 counting sort over the dense key space,
  *                2 bucketed counting sort (runs of 2^18 points or more)
- *   buckets      buckets of the bucketed counting sort (0 when it did not run)
- *   query_cells  cells below min_samples (one warp each in the core pass)
- *   border_cells cells holding a non-core point (one warp each in the label pass) */
+ *   buckets      buckets of the bucketed counting sort (0 when it did not run) */
 typedef struct dbs_run_stats {
   int64_t num_cells;
   int32_t key_bits;
@@ -192,9 +190,7 @@ typedef struct dbs_run_stats {
   int32_t sort_form;
   int32_t buckets;
   int64_t queries;
-  int64_t query_cells;
   int64_t border;
-  int64_t border_cells;
   int64_t pairs[2];
   int64_t warp_pairs[2];
 } dbs_run_stats;
