@@ -67,21 +67,19 @@ WORKLOAD = "constant_density_10M"
 DATA = "synthetic (seeded constant-density Gaussian blobs + 2% noise)"
 L2_FLUSH_BYTES = 512 << 20
 # Kernel launches of one dbscan2d call (tests/test_launch_count.py counts them
-# with the profiler): init, bounds, seg_finalize | bkt_part, bkt_local,
-# csort_clear, csort_count, csort, keys, radix | rle | cell_prep, huge_bbox |
-# core, status | 2 x (pairs, pair_scan, pair_warp) + flatten | ids, cid |
-# labels. Kernels whose work the device-side plan skips (the sort forms that
-# do not run, the huge-cell pass without huge cells) still launch and return
-# at once.
-KERNELS_PER_CALL = 25
+# with the profiler): init, bounds, seg_finalize | csort_clear, csort_count,
+# csort, keys, radix | rle | cell_prep, huge_bbox | core, status |
+# 2 x (pairs, pair_scan, pair_warp) + flatten | ids, cid | labels. Kernels
+# whose work the device-side plan skips (the sort form that does not run,
+# the huge-cell pass without huge cells) still launch and return at once.
+KERNELS_PER_CALL = 23
 # Launches per reference stage (the profile entry point times stages).
-STAGE_LAUNCHES = {"cell_keys": 3, "sort_gather": 7, "boundary_scan": 1, "build_ngh": 2,
+STAGE_LAUNCHES = {"cell_keys": 3, "sort_gather": 5, "boundary_scan": 1, "build_ngh": 2,
                   "core_mark": 2, "union_find": 7, "cluster_id": 2, "border_assign": 1}
 # The kernels that do a stage's work on this workload (the others of the
 # stage return at once); the sort's depend on the form that ran.
-SORT_KERNELS = {0: ("k_keys", "k_radix"), 1: ("k_csort_clear", "k_csort_count", "k_csort"),
-                2: ("k_bkt_part", "k_bkt_local")}
-SORT_FORM_NAME = {0: "radix", 1: "counting", 2: "bucketed counting"}
+SORT_KERNELS = {0: ("k_keys", "k_radix"), 1: ("k_csort_clear", "k_csort_count", "k_csort")}
+SORT_FORM_NAME = {0: "radix", 1: "counting"}
 STAGE_KERNEL = {"build_ngh": ("k_cell_prep",), "core_mark": ("k_core",),
                 "border_assign": ("k_labels",)}
 PROFILE_MD = os.path.join(ROOT, "profiles", "kernels_constant_density_10M.md")
@@ -507,7 +505,7 @@ def run_ours(args, world, rank, local):
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
            "data": DATA, "config": base_config(world),
            "pipeline": {"num_cells": cells, "key_bits": info["key_bits"], "radix_passes": passes,
-                        "sort": SORT_FORM_NAME[form], "buckets": info["buckets"],
+                        "sort": SORT_FORM_NAME[form],
                         "queries": info["queries"], "border_points": info["border"],
                         "union_pairs": [info["pairs_ring0"], info["pairs_ring1"]],
                         "union_warp_pairs": [info["warp_pairs_ring0"], info["warp_pairs_ring1"]]},

@@ -44,8 +44,7 @@ NVCC_FLAGS = [
     "-I", INCLUDE,
 ]
 
-CU_SOURCES = ["dbs_sort.cu", "dbs_csort.cu", "dbs_bsort.cu", "dbs_cells.cu", "dbs_cluster.cu",
-              "dbs_capi.cu"]
+CU_SOURCES = ["dbs_sort.cu", "dbs_csort.cu", "dbs_cells.cu", "dbs_cluster.cu", "dbs_capi.cu"]
 
 
 def _newer(target: str, deps: list[str]) -> bool:

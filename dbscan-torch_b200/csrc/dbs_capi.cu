@@ -95,15 +95,6 @@ size_t carve(int64_t n, int32_t nseg, char* base, Plan* p) {
   q.hot_cnt = cv.take<uint32_t>((size_t)kHotSlots);
   q.hot_cold = cv.take<uint32_t>((size_t)kHotSlots);
   q.hot_base = cv.take<uint32_t>((size_t)kHotSlots);
-  // Bucketed counting sort tables: only runs of kBktMinPoints points or more
-  // take that sort, so smaller runs (the built-in scratch form among them)
-  // carry none.
-  if (n >= kBktMinPoints) {
-    q.bkt_mat = cv.take<uint32_t>((size_t)kBktMaxBuckets * kBktMaxChunks);
-    q.bkt_tot = cv.take<uint32_t>((size_t)kBktMaxBuckets);
-    q.bkt_start = cv.take<uint32_t>((size_t)kBktMaxBuckets + 1);
-    q.bkt_status = cv.take<unsigned long long>((size_t)kBktMaxBuckets);
-  }
   q.n = n;
   q.nseg = nseg;
   q.scan_tiles = scan_tiles;
@@ -170,8 +161,7 @@ int run_pipeline(const Plan& p, cudaStream_t s, cudaEvent_t* evs) {
   if ((e = mark(0)) != cudaSuccess) return to_code(e);
   if ((e = launch_front(p, s)) != cudaSuccess) return to_code(e);            // cell_keys
   if ((e = mark(1)) != cudaSuccess) return to_code(e);
-  if ((e = launch_bsort(p, s)) != cudaSuccess) return to_code(e);            // sort_gather
-  if ((e = launch_csort(p, s)) != cudaSuccess) return to_code(e);
+  if ((e = launch_csort(p, s)) != cudaSuccess) return to_code(e);            // sort_gather
   if ((e = launch_keys(p, s)) != cudaSuccess) return to_code(e);
   if ((e = launch_radix(p, s)) != cudaSuccess) return to_code(e);
   if ((e = mark(2)) != cudaSuccess) return to_code(e);
@@ -507,7 +497,6 @@ int dbs_read_stats(const void* ws, void* stream, dbs_run_stats* out) {
   out->key_bytes = h.key64 ? 8 : 4;
   out->hot_slots = (int32_t)h.hot_used;
   out->sort_form = (int32_t)h.dense_sort;
-  out->buckets = h.dense_sort == 2u ? (int32_t)h.bkt_nb : 0;
   out->queries = h.q_count;
   out->border = h.b_count;
   // The flatten between the passes saved pass 0's counts; pass 1's are the

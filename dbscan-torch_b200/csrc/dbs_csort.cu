@@ -343,7 +343,7 @@ __global__ void __launch_bounds__(kCsThreads, 6) k_csort_count(Plan p) {
 __global__ void __launch_bounds__(kCsThreads, 5) k_csort(Plan p) {
   __shared__ uint32_t s_a[kCsThreads / 32], s_b[kCsThreads / 32];
   Desc* d = p.desc;
-  if (d->dense_sort != 1u) return;  // radix sort, or the bucketed sort ran
+  if (d->dense_sort != 1u) return;  // the radix sort ran
   const int64_t n = p.n;
   const int64_t W = (int64_t)d->dense_total;
   uint32_t* bins = p.bin_count;

@@ -67,22 +67,6 @@ constexpr int kHotSlots = 64;
 constexpr uint32_t kHotGroup = 8;
 constexpr int64_t kDenseSlack = 4096;
 
-// Bucketed counting sort (dbs_bsort.cu), for dense key spaces of runs with
-// at least kBktMinPoints points: the key space is cut into at most
-// kBktMaxBuckets buckets of 2^bkt_shift <= kBktMaxKeys consecutive keys; a
-// partition pass moves every point into its bucket's run, a local pass
-// counting-sorts each bucket in shared memory. A bucket holding more than
-// kBktCap points (a few huge cells) sends the run to the global counting
-// sort instead, whose hot-key path handles them.
-constexpr int kBktMaxBuckets = 4096;
-constexpr int kBktMaxKeys = 4096;
-constexpr int kBktMaxChunks = 1024;     // blocks of the cooperative partition
-constexpr int64_t kBktMinPoints = 1 << 18;
-constexpr uint32_t kBktCap = 1u << 16;
-constexpr int kBktTile = 4096;          // points per partition tile
-constexpr int kBktThreads = 256;
-constexpr int kBktTargetBuckets = 2048;  // buckets aimed at (fewer keys per bucket)
-
 // Grid-stride kernels whose grid (blocks per SM) a launch shape may set
 // (dbs_launch_shape of the C-ABI, same indices), and their built-in grids.
 // The label pass takes 32 blocks per SM while its border items go first
@@ -129,7 +113,6 @@ enum : int {
   kCtrLabels,
   kCtrBig,
   kCtrDebug,
-  kCtrBkt,
   kNumCtr
 };
 
@@ -178,16 +161,12 @@ struct Desc {
   unsigned long long big_packed;  // huge cells: entries << 40 | chunks
   uint32_t ctr[kNumCtr];
   uint32_t digit_total[2][kRadix];  // per-pass digit totals (ping-pong)
-  uint32_t dense_sort;  // 1: counting sort over the dense key space, 2: bucketed counting sort
+  uint32_t dense_sort;  // 1: counting sort over the dense key space
   uint32_t q_count;     // core-query list length (points of cells below ms)
   uint32_t b_count;     // border list length (non-core points)
   uint32_t p_count;     // union-find candidate pair list length
   uint32_t d_count;     // pairs deferred to warp-cooperative scans
   uint32_t hot_used;    // counting sort: occupied hot-key slots
-  uint32_t bkt_ok;      // bucketed sort possible (dense, enough points, buckets fit)
-  uint32_t bkt_shift;   // log2 keys per bucket
-  uint32_t bkt_nb;      // buckets
-  uint32_t bkt_max;     // points in the largest bucket
   uint32_t ring_pairs[2];  // p_count of each union pass (kept for the stats read-back)
   uint32_t ring_warp[2];   // d_count of each union pass
   GridBar bar;
@@ -243,11 +222,6 @@ struct Plan {
   uint32_t* hot_cnt;      //   points of hot rows per hot key
   uint32_t* hot_cold;     //   points of the key outside hot rows
   uint32_t* hot_base;     //   first sorted position of the key's hot points
-  uint32_t* bkt_mat;      // bucketed sort: per-(bucket, chunk) counts -> offsets, bucket-major
-                          //   (nullptr when n < kBktMinPoints: path disabled)
-  uint32_t* bkt_tot;      //   points per bucket (kBktMaxBuckets)
-  uint32_t* bkt_start;    //   first record of each bucket (kBktMaxBuckets + 1)
-  unsigned long long* bkt_status;  // look-back words of the local pass (kBktMaxBuckets)
   int32_t force_radix;    // debug entry: stable radix sort (reference perm)
   int64_t n;
   int32_t nseg;
@@ -349,19 +323,6 @@ __device__ __forceinline__ int32_t seg_of_key(const Plan& p, uint64_t b) {
     if (p.seg_info[mid].base <= b) lo = mid; else hi = mid - 1;
   }
   return lo;
-}
-
-// Bucket width of a dense key space of W keys: the fewest keys per bucket
-// (a power of two) that keeps the buckets at or below kBktTargetBuckets,
-// widened up to kBktMaxKeys; ~0 when even then more than kBktMaxBuckets
-// buckets would be needed.
-__device__ __forceinline__ uint32_t bkt_shift_for(uint64_t W, uint32_t* nb) {
-  uint32_t sh = 0;
-  while ((1u << sh) < (uint32_t)kBktMaxKeys && ((W + (1ull << sh) - 1) >> sh) > (uint64_t)kBktTargetBuckets) ++sh;
-  const uint64_t buckets = (W + (1ull << sh) - 1) >> sh;
-  if ((1u << sh) > (uint32_t)kBktMaxKeys || buckets > (uint64_t)kBktMaxBuckets || buckets == 0) return ~0u;
-  *nb = (uint32_t)buckets;
-  return sh;
 }
 
 // Per-cloud scalars of the dense key of a point (its dense-map index, which
@@ -521,7 +482,6 @@ cudaError_t launch_front(const Plan& p, cudaStream_t s);      // init, bounds, f
 cudaError_t launch_keys(const Plan& p, cudaStream_t s);
 cudaError_t launch_radix(const Plan& p, cudaStream_t s);
 cudaError_t launch_csort(const Plan& p, cudaStream_t s);
-cudaError_t launch_bsort(const Plan& p, cudaStream_t s);
 cudaError_t launch_rle(const Plan& p, cudaStream_t s);
 cudaError_t launch_cell_prep(const Plan& p, cudaStream_t s);
 cudaError_t launch_core(const Plan& p, cudaStream_t s);

@@ -44,7 +44,6 @@ __global__ void k_init(Plan p) {
   if (tid == 0) {
     d->bar.count = 0; d->bar.gen = 0; d->dense_sort = 0;
     d->q_count = 0; d->b_count = 0; d->p_count = 0; d->d_count = 0; d->hot_used = 0;
-    d->bkt_ok = 0; d->bkt_max = 0;
     d->ring_pairs[0] = d->ring_pairs[1] = 0; d->ring_warp[0] = d->ring_warp[1] = 0;
   }
   for (int64_t i = tid; i < p.scan_tiles; i += stride) p.rle_status[i] = 0;
@@ -302,18 +301,6 @@ __global__ void __launch_bounds__(1024) k_seg_finalize(Plan p) {
     d->dense_sort = (s_pooled || (!p.force_radix && !s_sparse && !s_overflow && dt < (1ull << 31)))
                         ? 1u : 0u;
     if (s_overflow) set_error(d, kErrKeySpace);
-    // Bucketed counting sort (dbs_bsort.cu) for runs with enough points
-    // whose key space splits into few enough buckets.
-    d->bkt_ok = 0;
-    if (d->dense_sort == 1u && p.bkt_mat != nullptr && p.n >= kBktMinPoints) {
-      uint32_t nb = 0;
-      const uint32_t sh = bkt_shift_for(dt, &nb);
-      if (sh != ~0u) {
-        d->bkt_ok = 1;
-        d->bkt_shift = sh;
-        d->bkt_nb = nb;
-      }
-    }
   }
 }
 

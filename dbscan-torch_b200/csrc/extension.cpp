@@ -509,7 +509,7 @@ std::map<std::string, int64_t> stats_dict(const void* ws, cudaStream_t stream) {
   check_rc(dbs_read_stats(ws, stream, &rs), "read_stats");
   return {{"num_cells", rs.num_cells}, {"key_bits", rs.key_bits}, {"passes", rs.passes},
           {"key_bytes", rs.key_bytes}, {"hot_slots", rs.hot_slots}, {"sort_form", rs.sort_form},
-          {"buckets", rs.buckets}, {"queries", rs.queries}, {"border", rs.border},
+          {"queries", rs.queries}, {"border", rs.border},
           {"pairs_ring0", rs.pairs[0]}, {"pairs_ring1", rs.pairs[1]},
           {"warp_pairs_ring0", rs.warp_pairs[0]}, {"warp_pairs_ring1", rs.warp_pairs[1]}};
 }
@@ -568,7 +568,7 @@ PYBIND11_MODULE(_C, m) {
   m.def("workspace_bytes", &workspace_bytes, pybind11::arg("n"), pybind11::arg("nseg") = 1);
   m.def("read_status", &read_status, pybind11::arg("ws"));
   m.def("read_stats", &read_stats, pybind11::arg("ws"),
-        "Work counts of the last run on a workspace (cells, sort form, buckets, queries, pairs).");
+        "Work counts of the last run on a workspace (cells, sort form, queries, border points, pairs).");
   m.def("dbscan2d_info", &dbscan2d_info, pybind11::arg("X"), pybind11::arg("eps"),
         pybind11::arg("min_samples"), "Labels plus the pipeline's shape and work counts (cells, key bits, passes, hot-key slots, "
         "queries, border points, union-find pairs per pass).");

@@ -137,7 +137,7 @@ class BatchedPlan:
         return self.labels
 
     def stats(self) -> dict:
-        """Work counts of the last run (cells, sort form, buckets, core
+        """Work counts of the last run (cells, sort form, hot-key slots, core
         queries, border points, union-find pairs); synchronises."""
         return dict(_C.read_stats(self.ws))
 

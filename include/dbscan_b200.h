@@ -178,9 +178,8 @@ int dbs_read_plan(const void* ws, void* stream, int64_t* num_cells, int32_t* key
  *   pairs[r]     candidate core-cell pairs listed by union pass r (0: side
  *                neighbours, 1: diagonal and outer ring)
  *   warp_pairs[r] of those, pairs scanned warp-cooperatively (over budget)
- *   sort_form    0 radix sort, 1 counting sort over the dense key space,
- *                2 bucketed counting sort (runs of 2^18 points or more)
- *   buckets      buckets of the bucketed counting sort (0 when it did not run) */
+ *   sort_form    0 radix sort (sparse key space, or the debug entry's stable
+ *                sort), 1 counting sort over the dense key space */
 typedef struct dbs_run_stats {
   int64_t num_cells;
   int32_t key_bits;
@@ -188,7 +187,6 @@ typedef struct dbs_run_stats {
   int32_t key_bytes;
   int32_t hot_slots;
   int32_t sort_form;
-  int32_t buckets;
   int64_t queries;
   int64_t border;
   int64_t pairs[2];

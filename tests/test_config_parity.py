@@ -44,14 +44,12 @@ def _cloud(kind: str, n: int) -> np.ndarray:
 
 
 # name, generator kind, points, eps, min_samples, sort form expected
-# (1: counting sort over the dense key space, 2: bucketed counting sort; the
-# adversarial cloud's 2M-point square overfills its bucket, so it takes the
-# global counting sort and its hot-key path)
+# (1: counting sort over the dense key space; every workload here is dense)
 WORKLOADS = [
     ("blobs_100k", "blobs", 100_000, 0.5, 10, 1),
-    ("constant_density_1M", "constant_density", 1_000_000, 0.5, 10, 2),
-    ("constant_density_5M", "constant_density", 5_000_000, 0.5, 10, 2),
-    ("constant_density_10M", "constant_density", 10_000_000, 0.5, 10, 2),
+    ("constant_density_1M", "constant_density", 1_000_000, 0.5, 10, 1),
+    ("constant_density_5M", "constant_density", 5_000_000, 0.5, 10, 1),
+    ("constant_density_10M", "constant_density", 10_000_000, 0.5, 10, 1),
     ("adversarial_4M_ms4", "adversarial", 4_000_000, 0.5, 4, 1),
     ("adversarial_4M_ms32", "adversarial", 4_000_000, 0.5, 32, 1),
 ]

@@ -66,15 +66,14 @@ def test_counting_sort_intermediates(name, X, eps, ms):
     _check_unstable_intermediates(name, X, Xd, eps, ms)
 
 
-@pytest.mark.parametrize("n,ms", [(1_000_000, 10), (400_000, 3)])
-def test_bucketed_sort_intermediates(n, ms):
-    """Clouds of 2^18 points or more take the bucketed counting sort: the same
-    order-free intermediates as the oracle's."""
+@pytest.mark.parametrize("n", [1_000_000, 400_000])
+def test_counting_sort_intermediates_large(n):
+    """The same order-free checks on clouds of 10^5 - 10^6 points."""
     X = synthetic.constant_density(n, seed=4) if n >= 10**6 else datasets.dense_overlapping_blobs(n, 3)
     Xd = torch.from_numpy(X).cuda()
-    _, info = _C.dbscan2d_info(Xd, 0.5, ms)
-    assert info["sort_form"] == 2, info
-    _check_unstable_intermediates(f"bucketed_{n}", X, Xd, 0.5, ms)
+    _, info = _C.dbscan2d_info(Xd, 0.5, 10)
+    assert info["sort_form"] == 1, info
+    _check_unstable_intermediates(f"dense_{n}", X, Xd, 0.5, 10)
 
 
 def _check_unstable_intermediates(name, X, Xd, eps, ms):

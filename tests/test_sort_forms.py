@@ -68,13 +68,11 @@ def test_batched_pooled_budget():
     off = np.concatenate([[0], np.cumsum([len(c) for c in clouds])])
     Xd = torch.from_numpy(X).cuda()
     lab = dbscan2d_batched(Xd, off.tolist(), 0.5, 4).cpu().numpy()
-    # The same batch through a plan: 601,500 points over one pooled map take
-    # the bucketed counting sort, with the records carrying their keys (more
-    # than one cloud per bucket).
+    # The same batch through a plan: one pooled map, the counting sort.
     plan = BatchedPlan(off.tolist())
     assert np.array_equal(plan.run(Xd, 0.5, 4).cpu().numpy(), lab)
     st = plan.stats()
-    assert st["sort_form"] == 2 and st["buckets"] > 0, st
+    assert st["sort_form"] == 1, st
     for k, c in enumerate(clouds):
         want = oracle.dbscan2d(c, 0.5, 4)
         assert np.array_equal(lab[off[k]:off[k + 1]], want), f"cloud {k}"
@@ -147,8 +145,6 @@ def test_hot_keys(order):
     the count pass through a 64-slot table. Points in cell order make nearly
     every row hot, so the table fills and later keys stay cold; a cloud with
     most points in one cell keeps one key hot. Labels equal the oracle's."""
-    # Fewer than 2^18 points: the global counting sort (with its hot-key
-    # table) runs, not the bucketed one.
     if order == "cell_order":
         X = synthetic.constant_density(250_000, seed=8)
         inv_r = np.float32(np.sqrt(np.float32(2.0)) / np.float32(EPS))
@@ -163,7 +159,7 @@ def test_hot_keys(order):
         X = X[rng.permutation(X.shape[0])]
         ms = 4
     ours, info = _C.dbscan2d_info(torch.from_numpy(X).cuda(), EPS, ms)
-    assert info["sort_form"] == 1, info  # the global counting sort ran
+    assert info["sort_form"] == 1, info  # the counting sort ran
     if order == "cell_order":
         # Nearly every row is hot: all 64 slots are taken and later hot keys
         # find their probe window full and stay cold.
