@@ -64,6 +64,7 @@ UNIT = "Mpoints/s"
 N_POINTS = 10_000_000
 EPS, MIN_SAMPLES = 0.5, 10
 WORKLOAD = "constant_density_10M"
+GENERATOR = "constant_density"
 DATA = "synthetic (seeded constant-density Gaussian blobs + 2% noise)"
 L2_FLUSH_BYTES = 512 << 20
 # Kernel launches of one dbscan2d call (tests/test_launch_count.py counts them
@@ -395,7 +396,7 @@ def run_reference(args, world, rank):
 # ----------------------------------------------------------------- our arm
 def run_ours(args, world, rank, local):
     syn = _synthetic()
-    X_np = syn.constant_density(N_POINTS, seed=rank)
+    X_np = getattr(syn, GENERATOR)(N_POINTS, seed=rank)
 
     # Baseline legs first, each in a fresh child process, before this process
     # touches the GPU or loads this build.
@@ -521,7 +522,8 @@ def run_ours(args, world, rank, local):
         if "ms_per_step" in rc:
             ref_lab = np.load(os.path.join(tmpdir, "ref_labels.npy"))
             rc["labels_equal"] = bool(np.array_equal(ref_lab, ours_labels))
-            rc["speedup"] = round(rc["ms_per_step"] / ms_mean, 2)
+            rc["speedup"] = round(rc["ms_per_step"] / ms_mean, 2)  # mean over mean, as `value`
+            rc["speedup_median"] = round(rc["median_ms"] / statistics.median(step_ms), 2)
         out["reference_cuda"] = rc
     if tmpdir is not None:
         import shutil
@@ -705,24 +707,35 @@ class RequestPool:
                 for i, (o, n) in enumerate(zip(off, sizes))]
 
 
-def _serve(srv, xs, arrivals, eps, ms):
+def _serve(srv, xs, arrivals, eps, ms, keep_every=0):
     """Offers the requests to the server at their arrival times (host
     clock); returns (latencies ms, clouds/s from the first arrival to the last
-    completion, batches)."""
+    completion, batches, {request index: labels} of every keep_every-th
+    request). Finished requests are released as they complete (a caller
+    holding every result would pin one label buffer per request)."""
     n = len(xs)
     srv.batches = srv.completed = 0
-    reqs = []
+    lat = np.empty(n)
+    kept = {}
+    pending = {}
     t0 = time.perf_counter()
+    t_last = t0
     i = 0
-    while i < n or srv.queue or any(l.busy for l in srv.lanes):
+    while i < n or pending:
         now = time.perf_counter() - t0
         while i < n and arrivals[i] <= now:
-            reqs.append(srv.submit(xs[i], float(eps[i]), int(ms[i]), t_submit=t0 + arrivals[i]))
+            pending[i] = srv.submit(xs[i], float(eps[i]), int(ms[i]), t_submit=t0 + arrivals[i])
             i += 1
         if srv.step() == 0:
             time.sleep(20e-6)
-    t_end = max(r.t_done for r in reqs) - t0
-    return np.array([r.latency for r in reqs]) * 1e3, n / t_end, srv.batches, reqs
+        else:
+            for k in [k for k, r in pending.items() if r.done]:
+                r = pending.pop(k)
+                lat[k] = r.latency * 1e3
+                t_last = max(t_last, r.t_done)
+                if keep_every and k % keep_every == 0:
+                    kept[k] = r.labels
+    return lat, n / (t_last - t0), srv.batches, kept
 
 
 def _plain(dbscan2d, xs, arrivals, eps, ms, keep_every=0):
@@ -774,10 +787,10 @@ def run_serving(dev, seconds: float, sweep_seconds: float) -> dict:
         pkg.dbscan2d(xs[k], float(eps[k]), int(ms[k]))
 
     arr, xs, eps, ms, sizes = stream(SERVE_RATE_HZ, seconds, 0)
-    lat_s, cps_s, batches, reqs = _serve(srv, xs, arr, eps, ms)
+    lat_s, cps_s, batches, kept_s = _serve(srv, xs, arr, eps, ms, keep_every=97)
     lat_p, cps_p, kept = _plain(pkg.dbscan2d, xs, arr, eps, ms, keep_every=97)
-    equal = all(torch.equal(reqs[k].labels, lab) for k, lab in kept.items())
-    del reqs, kept
+    equal = kept.keys() == kept_s.keys() and all(torch.equal(kept_s[k], lab) for k, lab in kept.items())
+    del kept_s, kept
 
     def sweep(run_arm):
         steps = []
@@ -836,6 +849,10 @@ def main():
                     help="length of the config-4 serving stream (0 skips serving)")
     ap.add_argument("--serve-sweep-seconds", type=float, default=3.0,
                     help="length of each offered-rate step of the saturation sweep")
+    ap.add_argument("--workload", choices=["constant_density", "sparse_uniform"],
+                    default="constant_density",
+                    help="main workload generator (sparse_uniform: the radix-sort path, for "
+                         "profiler captures; the benchmark line is constant_density)")
     ap.add_argument("--points", type=int, default=N_POINTS,
                     help="points of the main constant-density workload (smaller clouds for "
                          "profiler captures; the benchmark line is the 10M-point cloud)")
@@ -843,8 +860,9 @@ def main():
     ap.add_argument("--points-file", help=argparse.SUPPRESS)
     ap.add_argument("--labels-out", help=argparse.SUPPRESS)
     args = ap.parse_args()
-    if args.points != N_POINTS:
-        globals().update(N_POINTS=int(args.points), WORKLOAD=f"constant_density_{int(args.points)}")
+    if args.points != N_POINTS or args.workload != "constant_density":
+        globals().update(N_POINTS=int(args.points), WORKLOAD=f"{args.workload}_{int(args.points)}",
+                         GENERATOR=args.workload)
     if args.leg:
         print(json.dumps(run_leg(args)), flush=True)
         return

@@ -60,6 +60,15 @@ def constant_density(n: int = 10_000_000, seed: int = 0, noise_frac: float = 0.0
     return X
 
 
+def sparse_uniform(n: int, seed: int = 0) -> np.ndarray:
+    """n points uniform over a square of side 3*sqrt(n): about 0.014 points per
+    cell at eps 0.5, a key range ~70 times the point count, so the pipeline
+    takes its radix sort (the profile workload of that path)."""
+    rng = np.random.default_rng(seed)
+    side = 3.0 * np.sqrt(n)
+    return rng.uniform(-side / 2, side / 2, size=(n, 2)).astype(np.float32)
+
+
 def adversarial(n: int = 4_000_000, seed: int = 0) -> np.ndarray:
     """Dense square at (-20, -20); 64 spirals on an 8 x 8 grid of centres
     10 apart starting at (0, 0); lattice at x >= 100. Components are >= 5
