@@ -354,6 +354,7 @@ __device__ __forceinline__ void set_error(Desc* d, uint32_t bits) {
   atomicOr(&d->status, bits);
 }
 
+
 // Relaxed device-scope 64-bit load/store for look-back words.
 __device__ __forceinline__ unsigned long long ld_relaxed(const unsigned long long* p) {
   unsigned long long v;
