@@ -37,8 +37,23 @@ __device__ __forceinline__ void rle_body(const Plan& p, K* s_keys, uint32_t* s_w
     if (tile >= p.scan_tiles) break;
     const int64_t base = tile * kScanTile;
     const int32_t valid = (int32_t)min((int64_t)kScanTile, n - base);
-    // Coalesced load into shared memory, then blocked reads.
-    for (int32_t j = threadIdx.x; j < valid; j += blockDim.x) s_keys[j + 1] = keys[base + j];
+    // Coalesced load into shared memory (a thread's loads in flight in two
+    // rounds of kScanItems / 2), then blocked reads.
+#pragma unroll 1
+    for (int r = 0; r < 2; ++r) {
+      constexpr int kHalf = kScanItems / 2;
+      K kv[kHalf];
+#pragma unroll
+      for (int k = 0; k < kHalf; ++k) {
+        const int32_t j = threadIdx.x + (r * kHalf + k) * kScanThreads;
+        if (j < valid) kv[k] = keys[base + j];
+      }
+#pragma unroll
+      for (int k = 0; k < kHalf; ++k) {
+        const int32_t j = threadIdx.x + (r * kHalf + k) * kScanThreads;
+        if (j < valid) s_keys[j + 1] = kv[k];
+      }
+    }
     if (threadIdx.x == 0) s_keys[0] = base > 0 ? keys[base - 1] : (K)0;
     __syncthreads();
     const int32_t j0 = threadIdx.x * kScanItems;

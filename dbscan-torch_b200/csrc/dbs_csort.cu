@@ -44,6 +44,11 @@ constexpr uint32_t kFullMask = 0xffffffffu;
 // atomics in flight per thread.
 constexpr int kU = 4;
 
+// Points per block of the cooperative kernel's grid (the grid grows with the
+// cloud up to the resident blocks; a small cloud runs on few blocks, so its
+// four grid barriers are cheap).
+constexpr int64_t kCsPointsPerBlock = 2048;
+
 // Warp aggregation of equal keys for the per-key atomics. __match_any_sync
 // groups lanes with equal keys, but its cost grows with the number of
 // distinct keys in the warp (about 7x a plain atomic's issue cost for 32
@@ -441,8 +446,8 @@ cudaError_t launch_csort(const Plan& p, cudaStream_t s) {
   if (e != cudaSuccess) return e;
   k_csort_clear<<<p.num_sms * 4, kCsThreads, 0, s>>>(p);
   k_csort_count<<<p.num_sms * p.bps[kTuneCount], kCsThreads, 0, s>>>(p);
-  int grid = p.num_sms * blocks_per_sm;
-  if (grid > kMaxGrid) grid = kMaxGrid;
+  const int grid = coop_grid((p.n + kCsPointsPerBlock - 1) / kCsPointsPerBlock, p.num_sms,
+                             p.num_sms * blocks_per_sm);
   Plan q = p;
   void* args[] = {&q};
   return cudaLaunchCooperativeKernel((const void*)k_csort, dim3(grid), dim3(kCsThreads), args, 0, s);

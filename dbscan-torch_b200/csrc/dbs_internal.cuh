@@ -457,6 +457,18 @@ __device__ __forceinline__ void grid_sync(GridBar* b, Desc* d) {
 // sets the attributes and stores the resident blocks per SM in b. The mutex
 // serialises host threads that launch at the same time.
 constexpr int kMaxDevices = 64;
+// Grid of a cooperative kernel: `want` blocks for its work, at least one
+// block per SM, at most the resident blocks (every block of a cooperative
+// launch must be resident). A grid barrier costs one atomic per block on one
+// counter plus the wait for the last block, so a run with little work keeps
+// its grid small rather than filling the GPU with idle blocks.
+inline int coop_grid(int64_t want, int num_sms, int resident) {
+  int64_t g = want < num_sms ? num_sms : want;
+  if (g > resident) g = resident;
+  if (g > kMaxGrid) g = kMaxGrid;
+  return (int)g;
+}
+
 struct PerDeviceBlocks {
   std::mutex mu;
   int blocks[kMaxDevices] = {0};

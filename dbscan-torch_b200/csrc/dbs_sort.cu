@@ -305,6 +305,10 @@ __global__ void __launch_bounds__(1024) k_seg_finalize(Plan p) {
 }
 
 // ---------------------------------------------------------------- k_keys
+// Points (keys) per thread whose loads are issued together in the key and
+// count passes.
+constexpr int kLoadBatch = 8;
+
 // Compacted cell keys, one block per sort chunk, plus the chunk's histogram
 // of the first digit (the count step of pass 0).
 template <typename K>
@@ -315,16 +319,30 @@ __device__ __forceinline__ void keys_body(const Plan& p, uint32_t (*h)[kRadix]) 
   const int64_t b1 = min(n, b0 + (int64_t)p.chunk_tiles * kSortTile);
   const uint32_t warp = threadIdx.x >> 5;
   int32_t seg = b0 < b1 ? seg_of(p, b0) : 0;
-  for (int64_t i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
-    while (i >= p.seg_off[seg + 1]) ++seg;
-    const SegInfo& g = p.seg_info[seg];
-    const float inv_r = p.seg_param[seg].inv_r;
-    const float2 v = p.X[i];
-    const uint64_t gx = compact_axis(cell_coord(v.x, inv_r), g.bx, g.px);
-    const uint64_t gy = compact_axis(cell_coord(v.y, inv_r), g.by, g.py);
-    const uint64_t key = g.base + (gx << g.ysh) + gy;
-    keys[i] = (K)key;
-    atomicAdd(&h[warp][key & (kRadix - 1)], 1u);
+  // kLoadBatch points per thread and round: their loads are in flight
+  // together (a small cloud has few chunks, so each thread's rounds are the
+  // kernel's critical path).
+  for (int64_t i0 = b0 + threadIdx.x; i0 < b1; i0 += (int64_t)blockDim.x * kLoadBatch) {
+    float2 v[kLoadBatch];
+#pragma unroll
+    for (int k = 0; k < kLoadBatch; ++k) {
+      const int64_t i = i0 + (int64_t)k * blockDim.x;
+      if (i < b1) v[k] = p.X[i];
+    }
+#pragma unroll
+    for (int k = 0; k < kLoadBatch; ++k) {
+      const int64_t i = i0 + (int64_t)k * blockDim.x;
+      if (i < b1) {
+        while (i >= p.seg_off[seg + 1]) ++seg;
+        const SegInfo& g = p.seg_info[seg];
+        const float inv_r = p.seg_param[seg].inv_r;
+        const uint64_t gx = compact_axis(cell_coord(v[k].x, inv_r), g.bx, g.px);
+        const uint64_t gy = compact_axis(cell_coord(v[k].y, inv_r), g.by, g.py);
+        const uint64_t key = g.base + (gx << g.ysh) + gy;
+        keys[i] = (K)key;
+        atomicAdd(&h[warp][key & (kRadix - 1)], 1u);
+      }
+    }
   }
 }
 
@@ -375,8 +393,18 @@ __device__ __forceinline__ void count_body(const Plan& p, int pass, int32_t chun
   const uint32_t warp = threadIdx.x >> 5;
   for (int i = threadIdx.x; i < kSortWarps * kRadix; i += blockDim.x) (&h[0][0])[i] = 0;
   __syncthreads();
-  for (int64_t i = b0 + threadIdx.x; i < b1; i += blockDim.x)
-    atomicAdd(&h[warp][(uint32_t)((uint64_t)keys[i] >> shift) & (kRadix - 1)], 1u);
+  for (int64_t i0 = b0 + threadIdx.x; i0 < b1; i0 += (int64_t)blockDim.x * kLoadBatch) {
+    K kk[kLoadBatch];
+#pragma unroll
+    for (int k = 0; k < kLoadBatch; ++k) {
+      const int64_t i = i0 + (int64_t)k * blockDim.x;
+      kk[k] = i < b1 ? keys[i] : (K)0;
+    }
+#pragma unroll
+    for (int k = 0; k < kLoadBatch; ++k)
+      if (i0 + (int64_t)k * blockDim.x < b1)
+        atomicAdd(&h[warp][(uint32_t)((uint64_t)kk[k] >> shift) & (kRadix - 1)], 1u);
+  }
   __syncthreads();
   const uint32_t t = threadIdx.x;
   uint32_t sum = 0;
@@ -420,6 +448,39 @@ __device__ __forceinline__ void scan_body(const Plan& p, int pass, uint32_t dig,
     run += v[k];
   }
   __syncthreads();
+}
+
+// The same scan by one warp, for rows of at most kWarpScanChunks chunk
+// counts (4 per lane): a block scans kSortWarps digits at once, so a small
+// grid covers all kRadix digits in one step.
+constexpr int kWarpScanChunks = 128;
+
+__device__ __forceinline__ void scan_warp(const Plan& p, int pass, uint32_t dig) {
+  Desc* d = p.desc;
+  const uint32_t lane = lane_id();
+  uint32_t base = 0;
+  for (uint32_t t = lane; t < dig; t += 32) base += d->digit_total[pass & 1][t];
+  base = __reduce_add_sync(0xffffffffu, base);
+  uint32_t* row = p.chunk_count + (int64_t)dig * p.sort_chunks;
+  const int32_t b0 = lane * 4;
+  uint32_t v[4], sum = 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    v[k] = b0 + k < p.sort_chunks ? row[b0 + k] : 0u;
+    sum += v[k];
+  }
+  uint32_t x = sum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= (uint32_t)o) x += y;
+  }
+  uint32_t run = base + x - sum;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    if (b0 + k < p.sort_chunks) row[b0 + k] = run;
+    run += v[k];
+  }
 }
 
 __device__ __forceinline__ uint32_t digit_of(uint32_t key, uint32_t shift) {
@@ -563,8 +624,14 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_radix(Plan p) {
       }
       grid_sync(&d->bar, d);
     }
-    for (uint32_t dig = blockIdx.x; dig < (uint32_t)kRadix; dig += gridDim.x)
-      scan_body(p, pass, dig, sm.warp_tot_wide);
+    if (p.sort_chunks <= kWarpScanChunks) {
+      for (uint32_t dig = blockIdx.x * kSortWarps + (threadIdx.x >> 5); dig < (uint32_t)kRadix;
+           dig += gridDim.x * kSortWarps)
+        scan_warp(p, pass, dig);
+    } else {
+      for (uint32_t dig = blockIdx.x; dig < (uint32_t)kRadix; dig += gridDim.x)
+        scan_body(p, pass, dig, sm.warp_tot_wide);
+    }
     if (blockIdx.x == 0)
       for (int t = threadIdx.x; t < kRadix; t += blockDim.x) d->digit_total[(pass & 1) ^ 1][t] = 0;
     grid_sync(&d->bar, d);
@@ -602,7 +669,8 @@ cudaError_t launch_keys(const Plan& p, cudaStream_t s) {
 }
 
 // Cooperative launch: every block of the grid must be resident for the grid
-// barriers, so the grid is the occupancy-derived number of resident blocks.
+// barriers. One block per sort chunk (the count and scatter phases loop over
+// chunks), within the occupancy-derived number of resident blocks.
 cudaError_t launch_radix(const Plan& p, cudaStream_t s) {
   static PerDeviceBlocks cache;
   int blocks_per_sm = 0;
@@ -615,7 +683,7 @@ cudaError_t launch_radix(const Plan& p, cudaStream_t s) {
       },
       &blocks_per_sm);
   if (e != cudaSuccess) return e;
-  const int grid = p.num_sms * blocks_per_sm;
+  const int grid = coop_grid(p.sort_chunks, p.num_sms, p.num_sms * blocks_per_sm);
   Plan q = p;
   void* args[] = {&q};
   return cudaLaunchCooperativeKernel((const void*)k_radix, dim3(grid), dim3(kSortThreads), args,
