@@ -43,6 +43,7 @@ rank clusters its own cloud; the time is the max over ranks.
 from __future__ import annotations
 
 import argparse
+import gc
 import importlib.util
 import json
 import os
@@ -719,23 +720,25 @@ def _serve(srv, xs, arrivals, eps, ms, keep_every=0):
     lat = np.empty(n)
     kept = {}
     pending = {}
+    srv.pop_finished()
     t0 = time.perf_counter()
     t_last = t0
     i = 0
     while i < n or pending:
         now = time.perf_counter() - t0
         while i < n and arrivals[i] <= now:
-            pending[i] = srv.submit(xs[i], float(eps[i]), int(ms[i]), t_submit=t0 + arrivals[i])
+            r = srv.submit(xs[i], float(eps[i]), int(ms[i]), t_submit=t0 + arrivals[i])
+            pending[r.rid] = i
             i += 1
         if srv.step() == 0:
             time.sleep(20e-6)
         else:
-            for k in [k for k, r in pending.items() if r.done]:
-                r = pending.pop(k)
+            for r in srv.pop_finished():
+                k = pending.pop(r.rid)
                 lat[k] = r.latency * 1e3
                 t_last = max(t_last, r.t_done)
                 if keep_every and k % keep_every == 0:
-                    kept[k] = r.labels
+                    kept[k] = r.labels.clone()  # a view would hold its batch's block
     return lat, n / (t_last - t0), srv.batches, kept
 
 
@@ -761,6 +764,14 @@ def _pct(a, q):
     return round(float(np.percentile(a, q)), 3)
 
 
+def _tail(lat, arrivals):
+    """Where the slow requests were: how many took over the p99 bound, and
+    the arrival second of the slowest."""
+    k = int(np.argmax(lat))
+    return {"max_ms": round(float(lat[k]), 3), "max_at_s": round(float(arrivals[k]), 3),
+            "over_bound": int((lat > P99_BOUND_MS).sum())}
+
+
 def run_serving(dev, seconds: float, sweep_seconds: float) -> dict:
     """Config 4: Poisson arrivals at 2,000 req/s for `seconds`, sizes
     log-uniform in [1e3, 2e6] (config-0 clouds), eps U[0.1, 1.0], min_samples
@@ -776,7 +787,7 @@ def run_serving(dev, seconds: float, sweep_seconds: float) -> dict:
     syn = _synthetic()
     pool = RequestPool(dev)
     free0, total = torch.cuda.mem_get_info(dev)
-    srv = pkg.DbscanServer(budget_bytes=SERVE_BUDGET, lane_points=16 << 20, lane_clouds=256)
+    srv = pkg.DbscanServer(budget_bytes=SERVE_BUDGET, lane_points=16 << 20, lane_clouds=256, lanes=3)
 
     def stream(rate, dur, seed):
         arr, sizes, eps, ms, _ = syn.request_stream(rate_hz=rate, duration_s=dur, seed=seed)
@@ -790,6 +801,12 @@ def run_serving(dev, seconds: float, sweep_seconds: float) -> dict:
     _plain(pkg.dbscan2d, xs, arr, eps, ms)
 
     arr, xs, eps, ms, sizes = stream(SERVE_RATE_HZ, seconds, 0)
+    # The objects alive before the timed streams (the request views among
+    # them) move to the collector's permanent generation, so a full
+    # collection during a stream does not walk them: a serving process would
+    # freeze its start-up state the same way.
+    gc.collect()
+    gc.freeze()
     lat_s, cps_s, batches, kept_s = _serve(srv, xs, arr, eps, ms, keep_every=97)
     lat_p, cps_p, kept = _plain(pkg.dbscan2d, xs, arr, eps, ms, keep_every=97)
     equal = kept.keys() == kept_s.keys() and all(torch.equal(kept_s[k], lab) for k, lab in kept.items())
@@ -811,10 +828,13 @@ def run_serving(dev, seconds: float, sweep_seconds: float) -> dict:
         return {"capacity_clouds_per_s": good[-1]["achieved"] if good else 0.0,
                 "capacity_offered": good[-1]["offered"] if good else 0, "steps": steps}
 
+    gc.unfreeze()
     srv_arena = srv.arena_bytes
     sat_s = sweep(lambda x, a, e, m: _serve(srv, x, a, e, m)[:2])
     sat_p = sweep(lambda x, a, e, m: _plain(pkg.dbscan2d, x, a, e, m)[:2])
     pkg.check_status()
+    host_arena_mb = round(srv.host_arena.bytes / 2**20, 1) if srv.host_arena is not None else 0
+    host_fallbacks = srv.host_arena.fallbacks if srv.host_arena is not None else None
     del pool, srv
     torch.cuda.empty_cache()
     ratio = (sat_s["capacity_clouds_per_s"] / sat_p["capacity_clouds_per_s"]
@@ -825,11 +845,12 @@ def run_serving(dev, seconds: float, sweep_seconds: float) -> dict:
                         f"eps U[0.1, 1.0], min_samples U{{4..32}}",
             "requests": len(xs), "mean_points": round(float(np.mean(sizes)), 1),
             "budget_gb": round(SERVE_BUDGET / 2**30, 1), "free_hbm_gb": round(free0 / 2**30, 1),
-            "arena_gb": round(srv_arena / 2**30, 2),
+            "arena_gb": round(srv_arena / 2**30, 2), "host_arena_mb": host_arena_mb,
+            "host_arena_fallbacks": host_fallbacks,
             "server": {"p50_ms": _pct(lat_s, 50), "p99_ms": _pct(lat_s, 99),
-                       "clouds_per_s": round(cps_s, 1), "batches": batches},
+                       "clouds_per_s": round(cps_s, 1), "batches": batches, **_tail(lat_s, arr)},
             "sequential_plain": {"p50_ms": _pct(lat_p, 50), "p99_ms": _pct(lat_p, 99),
-                                 "clouds_per_s": round(cps_p, 1)},
+                                 "clouds_per_s": round(cps_p, 1), **_tail(lat_p, arr)},
             "labels_equal_sampled": bool(equal),
             "saturation": {"p99_bound_ms": P99_BOUND_MS, "step_seconds": sweep_seconds,
                            "server": sat_s, "sequential_plain": sat_p,
@@ -853,10 +874,11 @@ def main():
                     help="length of the config-4 serving stream (0 skips serving)")
     ap.add_argument("--serve-sweep-seconds", type=float, default=3.0,
                     help="length of each offered-rate step of the saturation sweep")
-    ap.add_argument("--workload", choices=["constant_density", "sparse_uniform"],
+    ap.add_argument("--workload", choices=["constant_density", "sparse_uniform", "blobs_with_noise"],
                     default="constant_density",
-                    help="main workload generator (sparse_uniform: the radix-sort path, for "
-                         "profiler captures; the benchmark line is constant_density)")
+                    help="main workload generator (sparse_uniform, or blobs_with_noise at small sizes: "
+                         "the radix-sort path, for profiler captures; the benchmark line is "
+                         "constant_density)")
     ap.add_argument("--points", type=int, default=N_POINTS,
                     help="points of the main constant-density workload (smaller clouds for "
                          "profiler captures; the benchmark line is the 10M-point cloud)")

@@ -21,7 +21,9 @@
 #include <torch/extension.h>
 
 #include <cstdlib>
+#include <iterator>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <utility>
@@ -473,6 +475,187 @@ void dbscan2d_batched_into(torch::Tensor X, torch::Tensor seg_offsets_dev, torch
            "dbscan2d_batched_into");
 }
 
+// Pinned host arena for served labels. Pinning host memory (cudaHostAlloc)
+// takes milliseconds per megabyte, and a caching pinned allocator pins a new
+// block whenever a batch needs a size it holds no free block of: under a
+// rising request rate those calls stalled the serving loop for up to 130 ms.
+// The arena pins its whole region once, at construction, and hands out
+// ranges of it first-fit; a range returns to the free list when the last
+// tensor viewing it is released (the tensor's deleter), coalescing with its
+// free neighbours. When no free range is large enough (results held for a
+// long time) the allocation falls back to the caching pinned allocator and
+// is counted.
+struct HostArenaState {
+  std::mutex mu;
+  char* base = nullptr;
+  size_t bytes = 0;
+  std::map<size_t, size_t> free_ranges;  // offset -> size
+  size_t in_use = 0;
+  int64_t fallbacks = 0;
+  ~HostArenaState() {
+    if (base != nullptr) cudaFreeHost(base);
+  }
+  void release(size_t off, size_t size) {
+    std::lock_guard<std::mutex> lock(mu);
+    in_use -= size;
+    auto it = free_ranges.emplace(off, size).first;
+    auto next = std::next(it);
+    if (next != free_ranges.end() && it->first + it->second == next->first) {
+      it->second += next->second;
+      free_ranges.erase(next);
+    }
+    if (it != free_ranges.begin()) {
+      auto prev = std::prev(it);
+      if (prev->first + prev->second == it->first) {
+        prev->second += it->second;
+        free_ranges.erase(it);
+      }
+    }
+  }
+};
+
+class PinnedArena {
+ public:
+  explicit PinnedArena(int64_t bytes) : st_(std::make_shared<HostArenaState>()) {
+    TORCH_CHECK(bytes > 0, "PinnedArena: bytes must be > 0");
+    const size_t b = ((size_t)bytes + kGrain - 1) & ~(kGrain - 1);
+    C10_CUDA_CHECK(cudaHostAlloc(reinterpret_cast<void**>(&st_->base), b, cudaHostAllocDefault));
+    st_->bytes = b;
+    st_->free_ranges.emplace(0, b);
+  }
+
+  // An int32 tensor of n elements in the arena, or from the caching pinned
+  // allocator when the arena has no free range that large.
+  torch::Tensor alloc_int32(int64_t n) {
+    const auto opts = torch::TensorOptions().dtype(torch::kInt32);
+    const size_t need = (((size_t)(n > 0 ? n : 1) * sizeof(int32_t)) + kGrain - 1) & ~(kGrain - 1);
+    size_t off = 0;
+    bool found = false;
+    {
+      std::lock_guard<std::mutex> lock(st_->mu);
+      for (auto it = st_->free_ranges.begin(); it != st_->free_ranges.end(); ++it) {
+        if (it->second < need) continue;
+        off = it->first;
+        const size_t rest = it->second - need;
+        st_->free_ranges.erase(it);
+        if (rest) st_->free_ranges.emplace(off + need, rest);
+        st_->in_use += need;
+        found = true;
+        break;
+      }
+      if (!found) ++st_->fallbacks;
+    }
+    if (!found) return torch::empty({n}, opts.pinned_memory(true));
+    std::shared_ptr<HostArenaState> st = st_;
+    return torch::from_blob(st_->base + off, {n}, [st, off, need](void*) { st->release(off, need); }, opts);
+  }
+
+  int64_t bytes() const { return (int64_t)st_->bytes; }
+  int64_t in_use() {
+    std::lock_guard<std::mutex> lock(st_->mu);
+    return (int64_t)st_->in_use;
+  }
+  int64_t fallbacks() {
+    std::lock_guard<std::mutex> lock(st_->mu);
+    return st_->fallbacks;
+  }
+
+ private:
+  static constexpr size_t kGrain = 256;
+  std::shared_ptr<HostArenaState> st_;
+};
+
+// Serving: one batch of host clouds through a lane's caller-owned device
+// buffers, enqueued on the current stream without synchronising: the cloud
+// table and parameter copies (from the lane's pinned staging tensors), one
+// host-to-device copy per cloud into the lane's point buffer, the segmented
+// pipeline, then one device-to-host copy of the batch's labels into a fresh
+// pinned int32 block (from `arena` when given, else from the caching pinned
+// allocator), and the device status word into status_host. Returns
+// one label tensor per cloud, each a view of that block (the block is freed
+// with the last view: clone a view to keep it alone). The per-cloud copies
+// are issued here rather than from Python so that a batch of a few hundred
+// clouds costs microseconds of host time, and one pinned block per batch
+// instead of one per cloud keeps the pinned allocations few. The caller keeps
+// every input tensor and the returned label tensors alive until the stream
+// has passed this batch (an event recorded after the call).
+std::vector<torch::Tensor> serve_launch(const std::vector<torch::Tensor>& xs, const std::vector<double>& eps,
+                                        const std::vector<int64_t>& min_samples, torch::Tensor X_dev,
+                                        torch::Tensor offsets_host, torch::Tensor offsets_dev,
+                                        torch::Tensor params_host, torch::Tensor params_dev,
+                                        torch::Tensor labels_dev, torch::Tensor ws, torch::Tensor status_host,
+                                        PinnedArena* arena) {
+  const int64_t S = (int64_t)xs.size();
+  TORCH_CHECK(S >= 1, "at least one cloud is required");
+  TORCH_CHECK((int64_t)eps.size() == S && (int64_t)min_samples.size() == S,
+              "eps and min_samples must have one entry per cloud");
+  TORCH_CHECK(X_dev.is_cuda() && offsets_dev.is_cuda() && params_dev.is_cuda() && labels_dev.is_cuda() &&
+                  ws.is_cuda(),
+              "the lane's buffers must be on CUDA");
+  TORCH_CHECK(offsets_host.is_pinned() && params_host.is_pinned() && status_host.is_pinned(),
+              "the lane's staging tensors must be pinned");
+  TORCH_CHECK(X_dev.is_contiguous() && X_dev.scalar_type() == torch::kFloat32 && X_dev.dim() == 2 &&
+                  X_dev.size(1) == 2,
+              "the lane's point buffer must be a contiguous float32 (P, 2) tensor");
+  TORCH_CHECK(labels_dev.scalar_type() == torch::kInt32 && labels_dev.numel() >= X_dev.size(0),
+              "the lane's label buffer must be int32 with one entry per point");
+  TORCH_CHECK(offsets_host.scalar_type() == torch::kInt64 && offsets_dev.scalar_type() == torch::kInt64 &&
+                  offsets_host.numel() >= S + 1 && offsets_dev.numel() >= S + 1,
+              "the lane's cloud tables hold fewer than len(xs) + 1 offsets");
+  TORCH_CHECK(params_host.numel() >= S * 16 && params_dev.numel() >= S * 16,
+              "the lane's parameter tables hold fewer than 16 bytes per cloud");
+  TORCH_CHECK(status_host.numel() * status_host.element_size() >= 4, "status_host must hold 4 bytes");
+  int64_t* off = offsets_host.data_ptr<int64_t>();
+  off[0] = 0;
+  for (int64_t k = 0; k < S; ++k) {
+    const torch::Tensor& x = xs[k];
+    TORCH_CHECK(!x.is_cuda() && x.dim() == 2 && x.size(1) == 2, "X must have shape (N, 2)");
+    TORCH_CHECK(x.scalar_type() == torch::kFloat32, "X must be float32");
+    TORCH_CHECK(x.is_contiguous(), "X must be contiguous");
+    TORCH_CHECK(eps[k] > 0.0, "eps must be > 0");
+    TORCH_CHECK(min_samples[k] >= 1, "min_samples must be >= 1");
+    off[k + 1] = off[k] + x.size(0);
+  }
+  const int64_t total = off[S];
+  TORCH_CHECK(total <= X_dev.size(0), "the batch holds ", total, " points, more than the lane's ",
+              X_dev.size(0));
+  check_rc(dbs_fill_seg_params(eps.data(), min_samples.data(), (int32_t)S, params_host.data_ptr()),
+           "serve_launch");
+  c10::cuda::CUDAGuard guard(X_dev.device());
+  cudaStream_t stream = at::cuda::getCurrentCUDAStream();
+  C10_CUDA_CHECK(cudaMemcpyAsync(offsets_dev.data_ptr(), off, (S + 1) * sizeof(int64_t),
+                                 cudaMemcpyHostToDevice, stream));
+  C10_CUDA_CHECK(cudaMemcpyAsync(params_dev.data_ptr(), params_host.data_ptr(), S * 16,
+                                 cudaMemcpyHostToDevice, stream));
+  float* xd = X_dev.data_ptr<float>();
+  for (int64_t k = 0; k < S; ++k) {
+    const int64_t n = xs[k].size(0);
+    if (n)
+      C10_CUDA_CHECK(cudaMemcpyAsync(xd + 2 * off[k], xs[k].data_ptr<float>(), n * 2 * sizeof(float),
+                                     cudaMemcpyHostToDevice, stream));
+  }
+  std::vector<torch::Tensor> out;
+  out.reserve(S);
+  const auto pinned = torch::TensorOptions().dtype(torch::kInt32).pinned_memory(true);
+  if (total == 0) {
+    for (int64_t k = 0; k < S; ++k) out.push_back(torch::empty({0}, pinned));
+    return out;
+  }
+  check_rc(dbs_dbscan2d_batched_device_shaped(xd, total, (int32_t)S, offsets_dev.data_ptr<int64_t>(),
+                                              params_dev.data_ptr(), labels_dev.data_ptr<int32_t>(),
+                                              ws.data_ptr(), ws.numel(), nullptr, stream),
+           "serve_launch");
+  // One pinned block for the whole batch, one copy out; each cloud's labels
+  // are a view of it (the block is released with the last of them).
+  auto block = arena != nullptr ? arena->alloc_int32(total) : torch::empty({total}, pinned);
+  C10_CUDA_CHECK(cudaMemcpyAsync(block.data_ptr<int32_t>(), labels_dev.data_ptr<int32_t>(),
+                                 total * sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
+  for (int64_t k = 0; k < S; ++k) out.push_back(block.narrow(0, off[k], off[k + 1] - off[k]));
+  C10_CUDA_CHECK(cudaMemcpyAsync(status_host.data_ptr(), ws.data_ptr(), sizeof(uint32_t),
+                                 cudaMemcpyDeviceToHost, stream));
+  return out;
+}
+
 std::vector<int64_t> default_launch_shape(int64_t n) {
   dbs_launch_shape sh{};
   check_rc(dbs_default_launch_shape(n, &sh), "default_launch_shape");
@@ -562,6 +745,21 @@ PYBIND11_MODULE(_C, m) {
         pybind11::arg("ws"), pybind11::arg("shape") = std::vector<int64_t>{},
         "Batched run on device-resident buffers (CUDA-graph capturable); shape: blocks per SM of the "
         "tuned kernels (empty = built-in).");
+  pybind11::class_<PinnedArena>(m, "PinnedArena",
+                                 "Pinned host memory pinned once and handed out in ranges (served labels).")
+      .def(pybind11::init<int64_t>(), pybind11::arg("bytes"))
+      .def("alloc_int32", &PinnedArena::alloc_int32, pybind11::arg("n"))
+      .def_property_readonly("bytes", &PinnedArena::bytes)
+      .def_property_readonly("in_use", &PinnedArena::in_use)
+      .def_property_readonly("fallbacks", &PinnedArena::fallbacks);
+  m.def("serve_launch", &serve_launch, pybind11::arg("xs"), pybind11::arg("eps"),
+        pybind11::arg("min_samples"), pybind11::arg("X_dev"), pybind11::arg("offsets_host"),
+        pybind11::arg("offsets_dev"), pybind11::arg("params_host"), pybind11::arg("params_dev"),
+        pybind11::arg("labels_dev"), pybind11::arg("ws"), pybind11::arg("status_host"),
+        pybind11::arg("arena") = nullptr,
+        "Serving: copies a batch of host clouds into a lane's device buffers, runs the batched "
+        "pipeline and copies the labels into one new pinned block, returning a view of it per cloud, "
+        "all on the current stream without synchronising.");
   m.def("default_launch_shape", &default_launch_shape, pybind11::arg("n"),
         "Built-in blocks per SM, for a run over n points, of the tuned kernels (count, cell_prep, core, pairs, pair_scan, labels).");
   m.def("fill_seg_params", &fill_seg_params, pybind11::arg("eps"), pybind11::arg("min_samples"));

@@ -51,7 +51,9 @@ extern "C" {
 #define DBS_STATUS_BARRIER 8u   /* a grid-wide barrier wait reached its cap */
 #define DBS_STATUS_CAPACITY 16u /* a work list (union-find cell pairs, at most 2^32 - 1)
                                    received more entries than it holds, or a sorted
-                                   position fell outside [0, n) (internal check) */
+                                   position fell outside [0, n) (internal check of
+                                   range only: two points sharing one position, or a
+                                   position left unfilled, would not set it) */
 
 #define DBS_NUM_STAGES 10
 

@@ -3,6 +3,8 @@ oracle's labels for that cloud (bit-exact) and a plain dbscan2d call on that
 cloud alone -- the same result alone and in the mix; admission respects the
 lane capacity and the device-memory budget; queued requests are batched."""
 
+import time
+
 import numpy as np
 import pytest
 import torch
@@ -81,3 +83,47 @@ def test_serve_admission():
     assert srv.batches >= 4
     want = torch.from_numpy(oracle.dbscan2d(X.numpy(), 0.5, 10))
     assert all(torch.equal(r.labels, want) for r in reqs)
+
+
+@pytest.mark.gpu
+def test_serve_pop_finished():
+    """pop_finished() hands back every completed request exactly once, each
+    with its labels, once a caller has asked for it."""
+    srv = DbscanServer(budget_bytes=1 << 30, lane_clouds=4, lanes=3)
+    assert srv.pop_finished() == []
+    reqs = [srv.submit(X, e, m) for X, e, m in _requests(25, 3)]
+    seen = []
+    t_end = time.monotonic() + 120.0
+    while len(seen) < len(reqs) and time.monotonic() < t_end:
+        srv.step()
+        seen.extend(srv.pop_finished())
+    assert sorted(r.rid for r in seen) == sorted(r.rid for r in reqs)
+    assert srv.pop_finished() == []
+    for r in seen:
+        assert r.done
+        _check(r)
+
+
+@pytest.mark.gpu
+def test_pinned_arena_reuse():
+    """The host arena hands out ranges first-fit, takes them back when the
+    last view is released (coalescing neighbours) and counts the
+    allocations it had to leave to torch's pinned allocator."""
+    a = _C.PinnedArena(1 << 20)
+    assert a.bytes == 1 << 20 and a.in_use == 0
+    x = a.alloc_int32(1000)
+    y = a.alloc_int32(50_000)
+    assert x.is_pinned() and y.is_pinned() and a.in_use >= 204_000
+    x.fill_(7)
+    v = x[10:20]
+    del x
+    assert a.in_use >= 200_000  # the view keeps its range
+    assert int(v.sum()) == 70
+    del v, y
+    assert a.in_use == 0
+    big = a.alloc_int32(1 << 18)  # the whole arena: the freed ranges coalesced
+    assert a.fallbacks == 0 and a.in_use == 1 << 20
+    z = a.alloc_int32(10)  # nothing left: torch's pinned allocator
+    assert a.fallbacks == 1 and z.is_pinned()
+    del big, z
+    assert a.in_use == 0
