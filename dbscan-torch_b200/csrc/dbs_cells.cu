@@ -292,11 +292,12 @@ __global__ void __launch_bounds__(kCellThreads, 5) k_cell_prep(Plan p) {
     // Neighbour row, off = (dx+2)*5 + (dy+2) as in the reference.
     if (valid) {
       const SegInfo g = p.seg_info[seg];  // in registers for the 25 lookups
-      const uint64_t local = p.cell_key[c] - g.base;
-      const uint64_t gx = local >> g.ysh;
-      const uint64_t gy = local & ((1ull << g.ysh) - 1ull);
-      const int32_t kx = expand_axis(gx, g.bx, g.px);
-      const int32_t ky = expand_axis(gy, g.by, g.py);
+      // The cell's grid coordinates, from its first point (the key was made
+      // from the same coordinates, so no division of the key is needed).
+      const float inv_r = p.seg_param[seg].inv_r;
+      const float2 v0 = p.xy[s0];
+      const int32_t kx = cell_coord(v0.x, inv_r);
+      const int32_t ky = cell_coord(v0.y, inv_r);
       uint64_t ngy[5];
 #pragma unroll
       for (int dy = 0; dy < 5; ++dy)
@@ -307,7 +308,7 @@ __global__ void __launch_bounds__(kCellThreads, 5) k_cell_prep(Plan p) {
 #pragma unroll
         for (int dx = 0; dx < 5; ++dx) {
           const uint64_t ngx = compact_axis((int32_t)((uint32_t)kx + (uint32_t)(dx - 2)), g.bx, g.px);
-          const int32_t* mrow = p.cell_map + g.map_base + (int64_t)(ngx << g.ysh);
+          const int32_t* mrow = p.cell_map + g.map_base + (int64_t)(ngx * g.ys);
 #pragma unroll
           for (int dy = 0; dy < 5; ++dy)
             r[dx * 5 + dy] = (ngx != ~0ull && ngy[dy] != ~0ull) ? mrow[ngy[dy]] : -1;
@@ -316,7 +317,7 @@ __global__ void __launch_bounds__(kCellThreads, 5) k_cell_prep(Plan p) {
         for (int k = 0; k < 25; ++k) srow[lane * kNgh + k] = r[k];
       } else {
         // Sparse cloud: its cells are sorted by key, and the five neighbours
-        // of one column (same gx) are the keys base + (ngx << ysh) + ngy[dy].
+        // of one column (same gx) are the keys base + ngx * ys + ngy[dy].
         // Taken in ascending ngy (a sorting network over the five, invalid
         // coordinates last), consecutive targets of one coordinate class are
         // one key apart, so each is reached from the previous one by a walk
@@ -346,7 +347,7 @@ __global__ void __launch_bounds__(kCellThreads, 5) k_cell_prep(Plan p) {
             for (int dy = 0; dy < 5; ++dy) out[dy] = -1;
             continue;
           }
-          const uint64_t rowbase = g.base + (ngx << g.ysh);
+          const uint64_t rowbase = g.base + ngx * g.ys;
           int64_t pos = key_lower_bound(p.cell_key, lo0, hi0, rowbase + sy[0]);
 #pragma unroll
           for (int j = 0; j < 5; ++j) {

@@ -130,9 +130,9 @@ struct SegParam {
 // non-negative and negative classes so that the compaction preserves the
 // reference's unsigned key order ((u32)kx << 32 | (u32)ky): non-negative
 // coordinates come first, then negative ones, each class ascending.
-// The compacted key of cell (gx, gy) is base + (gx << ysh) + gy with
-// ysh = ceil(log2(wy)): lexicographic in (gx, gy), and a cell's coordinates
-// come back from its key with a shift and a mask.
+// The compacted key of cell (gx, gy) is base + gx * wy + gy (mixed radix,
+// no padding of the y width to a power of two): lexicographic in (gx, gy),
+// and a cell's coordinates come back from its key with a division by wy.
 struct SegInfo {
   int32_t bx[4];     // x: lo_pos, hi_pos, lo_neg, hi_neg (atomics)
   int32_t by[4];     // y: same
@@ -141,7 +141,7 @@ struct SegInfo {
   uint64_t base;     // first global key of this cloud
   int64_t map_base;  // offset in the dense cell map, -1 when not dense
   int32_t cell_begin;  // first cell index of this cloud (filled by k_rle)
-  uint32_t ysh;      // bits of the y part of the local key
+  uint64_t ys;       // key stride of one x column: max(wy, 1)
 };
 
 // Software grid barrier of the cooperative kernels (all blocks resident).
@@ -308,11 +308,6 @@ __device__ __forceinline__ uint64_t compact_axis(int32_t k, const int32_t b[4], 
   return pw + (uint64_t)(uint32_t)(k - b[2]);
 }
 
-__device__ __forceinline__ int32_t expand_axis(uint64_t g, const int32_t b[4], uint64_t pw) {
-  if (g < pw) return (int32_t)((uint32_t)b[0] + (uint32_t)g);
-  return (int32_t)((uint32_t)b[2] + (uint32_t)(g - pw));
-}
-
 // Cloud owning global key b: the last cloud whose key base is <= b (empty
 // clouds share their base with the next cloud and come before it).
 __device__ __forceinline__ int32_t seg_of_key(const Plan& p, uint64_t b) {
@@ -329,8 +324,7 @@ __device__ __forceinline__ int32_t seg_of_key(const Plan& p, uint64_t b) {
 // fits 31 bits), held in registers while a thread's points stay in one cloud.
 struct KeyCtx {
   int32_t bx[4], by[4];
-  uint64_t px, py, base;
-  uint32_t ysh;
+  uint64_t px, py, base, ys;
   float inv_r;
   int64_t end;  // first input index past the cloud
   int32_t seg;
@@ -338,7 +332,7 @@ struct KeyCtx {
     const SegInfo& g = p.seg_info[s];
 #pragma unroll
     for (int k = 0; k < 4; ++k) { bx[k] = g.bx[k]; by[k] = g.by[k]; }
-    px = g.px; py = g.py; base = g.base; ysh = g.ysh;
+    px = g.px; py = g.py; base = g.base; ys = g.ys;
     inv_r = p.seg_param[s].inv_r;
     end = p.seg_off[s + 1];
     seg = s;
@@ -346,7 +340,7 @@ struct KeyCtx {
   __device__ uint32_t key(float2 v) const {
     const uint64_t gx = compact_axis(cell_coord(v.x, inv_r), bx, px);
     const uint64_t gy = compact_axis(cell_coord(v.y, inv_r), by, py);
-    return (uint32_t)(base + (gx << ysh) + gy);
+    return (uint32_t)(base + gx * ys + gy);
   }
 };
 

@@ -216,12 +216,12 @@ __global__ void __launch_bounds__(1024) k_seg_finalize(Plan p) {
       const uint64_t nny = g.by[2] < 0 ? (uint64_t)((int64_t)g.by[3] - g.by[2] + 1) : 0;
       g.px = npx; g.wx = npx + nnx;
       g.py = npy; g.wy = npy + nny;
-      g.ysh = g.wy <= 1 ? 0u : 64u - (uint32_t)__clzll((long long)(g.wy - 1));
+      g.ys = g.wy < 1 ? 1ull : g.wy;
       const int64_t npts = p.seg_off[s + 1] - p.seg_off[s];
       if (npts > 0) {
-        // range = wx << ysh, saturating (only one full-range cloud fits 64 bits)
-        if (g.ysh >= 64 || (g.ysh > 0 && g.wx > ((~0ull) >> g.ysh))) { sat = true; range = ~0ull; }
-        else range = g.wx << g.ysh;
+        // range = wx * ys, saturating (only one full-range cloud fits 64 bits)
+        if (g.wx > (~0ull) / g.ys) { sat = true; range = ~0ull; }
+        else range = g.wx * g.ys;
         const unsigned long long cap = (unsigned long long)(kDenseFactor * npts + kDenseSlack);
         if (!sat && range <= cap) dense = range;
         else atomicOr(&s_sparse, 1);
@@ -285,7 +285,7 @@ __global__ void __launch_bounds__(1024) k_seg_finalize(Plan p) {
     unsigned long long max_key = s_carry_range == 0 ? 0 : s_carry_range - 1;
     if (p.nseg == 1) {
       const SegInfo& g = p.seg_info[0];
-      max_key = (g.wx == 0 || g.wy == 0) ? 0 : ((g.wx - 1) << g.ysh) + (g.wy - 1);
+      max_key = (g.wx == 0 || g.wy == 0) ? 0 : (g.wx - 1) * g.ys + (g.wy - 1);
     }
     uint32_t nbits = max_key == 0 ? 0 : 64 - __clzll((long long)max_key);
     uint32_t np = (nbits + kRadixBits - 1) / kRadixBits;
@@ -338,7 +338,7 @@ __device__ __forceinline__ void keys_body(const Plan& p, uint32_t (*h)[kRadix]) 
         const float inv_r = p.seg_param[seg].inv_r;
         const uint64_t gx = compact_axis(cell_coord(v[k].x, inv_r), g.bx, g.px);
         const uint64_t gy = compact_axis(cell_coord(v[k].y, inv_r), g.by, g.py);
-        const uint64_t key = g.base + (gx << g.ysh) + gy;
+        const uint64_t key = g.base + gx * g.ys + gy;
         keys[i] = (K)key;
         atomicAdd(&h[warp][key & (kRadix - 1)], 1u);
       }
