@@ -574,7 +574,7 @@ def run_batched_sharded(dev, n_clouds: int, world: int, rank: int) -> dict:
 
 
 def run_batched(dev, n_clouds: int) -> dict:
-    """Config 3: n_clouds independent clouds (sizes log-uniform in [256, 262144],
+    """The batched workload: n_clouds independent clouds (sizes log-uniform in [256, 262144],
     eps_i in [0.2, 1.0], min_samples_i in {4..32}) clustered by one batched
     pipeline run, against a loop of plain calls over the same device-resident
     clouds. Both timed with CUDA events; labels compared cloud by cloud.
@@ -651,8 +651,8 @@ def graph_gaps(plan, graph_ms: float) -> dict:
 
 def run_configs(dev) -> dict:
     """The other plain-call workloads, device-resident, CUDA events around each
-    call (median of 7 after 3 warm-ups): config 0 (100k blobs with noise),
-    config 1 at 1M and 5M points, config 2 (adversarial 4M cloud, min_samples
+    call (median of 7 after 3 warm-ups): 100k blobs with noise, constant density
+    at 1M and 5M points, the adversarial 4M cloud (min_samples
     4 and 32)."""
     pkg = _package()
     syn = _synthetic()
@@ -687,11 +687,11 @@ SERVE_WARMUP_S = 3.0
 
 
 class RequestPool:
-    """Host-side request clouds of the config-0 distribution: `bases` clouds
+    """Host-side request clouds of the blobs-with-noise distribution: `bases` clouds
     of `base_n` points (20 blobs + 5% noise, shuffled; device generator, one
     seed per cloud) copied once to pinned host memory. Request i is the
     window of its size at a seeded random offset of base cloud i mod bases:
-    a random subsample of a shuffled config-0 cloud, so a config-0 cloud of
+    a random subsample of a shuffled blobs-with-noise cloud, so such a cloud of
     that size, and no two requests share their point set."""
 
     def __init__(self, dev, bases: int = 64, base_n: int = 2_000_000, seed: int = 1):
@@ -773,8 +773,8 @@ def _tail(lat, arrivals):
 
 
 def run_serving(dev, seconds: float, sweep_seconds: float) -> dict:
-    """Config 4: Poisson arrivals at 2,000 req/s for `seconds`, sizes
-    log-uniform in [1e3, 2e6] (config-0 clouds), eps U[0.1, 1.0], min_samples
+    """Serving: Poisson arrivals at 2,000 req/s for `seconds`, sizes
+    log-uniform in [1e3, 2e6] (blobs-with-noise clouds), eps U[0.1, 1.0], min_samples
     U{4..32}, through the continuous-batching server (admission under a 64 GiB
     budget, checked against free device memory) and through sequential plain
     calls, each arm after a SERVE_WARMUP_S warm-up stream at the same rate;
@@ -841,7 +841,7 @@ def run_serving(dev, seconds: float, sweep_seconds: float) -> dict:
              if sat_p["capacity_clouds_per_s"] else None)
     return {"workload": f"Poisson {SERVE_RATE_HZ:g} req/s for {seconds:g} s (after a {SERVE_WARMUP_S:g} s "
                         f"warm-up stream per arm), N log-uniform [1e3, 2e6] "
-                        f"(config-0 clouds: windows at random offsets of 64 shuffled 2M-point clouds), "
+                        f"(blobs-with-noise clouds: windows at random offsets of 64 shuffled 2M-point clouds), "
                         f"eps U[0.1, 1.0], min_samples U{{4..32}}",
             "requests": len(xs), "mean_points": round(float(np.mean(sizes)), 1),
             "budget_gb": round(SERVE_BUDGET / 2**30, 1), "free_hbm_gb": round(free0 / 2**30, 1),
@@ -871,7 +871,7 @@ def main():
     ap.add_argument("--batched-clouds", type=int, default=4096,
                     help="clouds of the batched comparison (0 skips it)")
     ap.add_argument("--serve-seconds", type=float, default=60.0,
-                    help="length of the config-4 serving stream (0 skips serving)")
+                    help="length of the serving stream (0 skips serving)")
     ap.add_argument("--serve-sweep-seconds", type=float, default=3.0,
                     help="length of each offered-rate step of the saturation sweep")
     ap.add_argument("--workload", choices=["constant_density", "sparse_uniform", "blobs_with_noise"],
