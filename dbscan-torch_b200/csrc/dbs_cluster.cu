@@ -40,13 +40,33 @@ __device__ __forceinline__ void append(uint32_t* list, uint32_t* count, bool tak
 __constant__ int8_t kNearFirst[24] = {7, 11, 13, 17, 6, 8, 16, 18, 2, 10, 14, 22,
                                       1, 3, 5, 9, 15, 19, 21, 23, 0, 4, 20, 24};
 
+// Neighbour cells whose row entry, box and point range one thread loads
+// together before it tests any of them (k_core, k_labels): the loads of a
+// group are independent, so a thread waits for one memory latency per group
+// instead of three dependent ones (row entry -> box -> point range) per cell.
+// Wider groups take more registers, hence fewer resident warps. Runs of up to
+// kSmallRun points are bound by their slowest threads' chains of dependent
+// loads and take the wide form; larger runs are bound by the loads in flight
+// across the GPU and take the narrow one (k_core groups of 2, k_labels one
+// cell at a time with its loads in program order). Measured on B200 against
+// one cell at a time for both: 1M constant-density points, k_core 19.4 ->
+// 15.9 us and k_labels 32.3 -> 18.5 us (groups of 4); 100k blobs, 16.5 ->
+// 12.6 and 23.2 -> 13.3 us; 10M points, k_core 76.3 -> 71.0 us (groups of
+// 2), while groups of 4 (46 and 58 registers) slowed k_core to 87.7 us and
+// k_labels from 111.2 to 150.3 us.
+constexpr int64_t kSmallRun = 2 << 20;
+constexpr int kNbGroupSmall = 4;
+constexpr int kNbGroupLarge = 2;
+
 // Core flag of every query point, one thread per query. A query counts its
 // own cell wholesale (the reference never distance-tests the centre cell,
 // :231-233) plus the points within eps of the other 24 stencil cells that
 // survive the point-box prune (:235-240), stopping once the count reaches
 // ms (k_core_pass2 :213-245). Queries that stay non-core go to the border
 // list of k_labels.
+template <int kNbGroup>
 __global__ void __launch_bounds__(kCellThreads) k_core(Plan p) {
+  static_assert((kNgh - 1) % kNbGroup == 0, "groups tile the 24 stencil neighbours");
   const uint32_t qn = p.desc->q_count;
   const uint32_t stride = gridDim.x * blockDim.x;
   for (uint32_t base = blockIdx.x * blockDim.x; base < qn; base += stride) {
@@ -66,19 +86,31 @@ __global__ void __launch_bounds__(kCellThreads) k_core(Plan p) {
       // Nearest cells first, so the count reaches ms (and stops) sooner; a
       // neighbour cell wholly within eps of q (point_box_max_d2) counts all
       // its points without distance tests. Neither changes the core flag.
-      for (int o = 0; o < kNgh - 1 && cnt < ms; ++o) {
-        const int32_t nb = row[kNearFirst[o]];
-        if (nb < 0) continue;
-        const float4 bb = p.bbox[nb];
-        if (!(point_box_d2(q.x, q.y, bb) <= eps_sq)) continue;
-        const int32_t j0 = p.cell_start[nb], j1 = p.cell_start[nb + 1];
-        if (point_box_max_d2(q.x, q.y, bb) <= eps_sq) {
-          cnt += j1 - j0;
-          continue;
+      for (int g = 0; g < kNgh - 1 && cnt < ms; g += kNbGroup) {
+        int32_t nb[kNbGroup], j0[kNbGroup], j1[kNbGroup];
+        float4 bb[kNbGroup];
+#pragma unroll
+        for (int u = 0; u < kNbGroup; ++u) nb[u] = row[kNearFirst[g + u]];
+#pragma unroll
+        for (int u = 0; u < kNbGroup; ++u) {
+          const int32_t s = max(nb[u], 0);  // cell 0 exists: this cloud has cell c
+          bb[u] = p.bbox[s];
+          j0[u] = p.cell_start[s];
+          j1[u] = p.cell_start[s + 1];
         }
-        for (int32_t j = j0; j < j1; ++j) {
-          const float2 pj = p.xy[j];
-          cnt += sq_dist(__fsub_rn(pj.x, q.x), __fsub_rn(pj.y, q.y)) <= eps_sq;
+#pragma unroll
+        for (int u = 0; u < kNbGroup; ++u) {
+          if (nb[u] < 0 || cnt >= ms) continue;
+          if (!(point_box_d2(q.x, q.y, bb[u]) <= eps_sq)) continue;
+          if (point_box_max_d2(q.x, q.y, bb[u]) <= eps_sq) {
+            cnt += j1[u] - j0[u];
+            continue;
+          }
+#pragma unroll 4
+          for (int32_t j = j0[u]; j < j1[u]; ++j) {
+            const float2 pj = p.xy[j];
+            cnt += sq_dist(__fsub_rn(pj.x, q.x), __fsub_rn(pj.y, q.y)) <= eps_sq;
+          }
         }
       }
       const bool core = cnt >= ms;
@@ -229,8 +261,8 @@ __constant__ int8_t kRingOffs[2][kPassOffs] = {
 // that most of its pairs are already connected):
 //   k_pairs       one thread per core cell: its neighbours nc > c of the
 //                 pass that are core cells and pass the box-box prune
-//                 (dbscan_cuda.cu:329-351); with `skip_united` (after a
-//                 flatten) pairs already in one component are dropped.
+//                 (dbscan_cuda.cu:329-351); in pass 1 (after a flatten)
+//                 pairs already in one component are dropped.
 //                 Survivors go to a pair list.
 //   k_pair_scan   one thread per listed pair: i over c's core points passing
 //                 the point-box prune against nc, j over nc's core points,
@@ -241,34 +273,54 @@ __constant__ int8_t kRingOffs[2][kPassOffs] = {
 // Whether an edge exists does not depend on the order of the tests, and the
 // components (rooted at their smallest cell) do not depend on the order of
 // the unions, so the labels are those of the reference.
-__global__ void __launch_bounds__(256) k_pairs(Plan p, int ring, int skip_united) {
+//
+// Loads are issued in independent batches of neighbours: their row entries,
+// then their status (and, in pass 1, their root), then the boxes of those
+// still in play, so a cell waits for three memory latencies per batch
+// instead of up to three per neighbour.
+template <int RING>
+__global__ void __launch_bounds__(256) k_pairs(Plan p) {
+  constexpr int nofs = RING == 0 ? 4 : kPassOffs;
+  constexpr int kPairsBatch = RING == 0 ? 4 : 5;  // neighbours whose loads go out together
+  static_assert(nofs % kPairsBatch == 0, "batches tile the pass's offsets");
   Desc* d = p.desc;
   const uint32_t C = d->num_cells;
-  const int nofs = ring == 0 ? 4 : kPassOffs;
   const uint32_t stride = gridDim.x * blockDim.x;
   for (uint32_t base = blockIdx.x * blockDim.x; base < C; base += stride) {
     const uint32_t c = base + threadIdx.x;
-    uint32_t mask = 0;  // candidate offsets (bit k = kRingOffs[ring][k])
+    uint32_t mask = 0;  // candidate offsets (bit k = kRingOffs[RING][k])
     const int32_t* row = p.ngh + (int64_t)min(c, C - 1) * kNgh;
     if (c < C && p.cell_status[c] != 0) {
       const float eps_sq = p.seg_param[p.cell_seg[c]].eps_sq;
       const float4 bb_c = p.bbox[c];
-      int32_t root_c = -1;
+      // Pass 1 runs after a flatten: every cell points at its root and no
+      // union runs during this kernel, so one load is the find. Pairs
+      // already in one component are dropped before their boxes are read
+      // (in dense regions most pass-1 neighbours are joined already).
+      const int32_t root_c = RING == 1 ? p.uf[c] : 0;  // r = -1 below never equals it
 #pragma unroll
-      for (int k = 0; k < kPassOffs; ++k) {
-        if (k >= nofs) continue;
-        const int32_t nb = row[kRingOffs[ring][k]];
-        if (nb <= (int32_t)c || p.cell_status[nb] == 0) continue;
-        if (skip_united) {
-          // The flatten just before left every cell pointing at its root,
-          // and no union runs during this kernel: one load is the find.
-          // Checked before the box (a 4-byte load against 16): in dense
-          // regions most pass-1 neighbours are joined already.
-          if (root_c < 0) root_c = p.uf[c];
-          if (p.uf[nb] == root_c) continue;
+      for (int h = 0; h < nofs; h += kPairsBatch) {
+        int32_t nb[kPairsBatch];
+#pragma unroll
+        for (int k = 0; k < kPairsBatch; ++k) nb[k] = row[kRingOffs[RING][h + k]];
+        bool any = false;
+#pragma unroll
+        for (int k = 0; k < kPairsBatch; ++k) any |= nb[k] > (int32_t)c;
+        if (!any) continue;  // no neighbour above c in this batch (sparse regions)
+        uint32_t m = 0;
+#pragma unroll
+        for (int k = 0; k < kPairsBatch; ++k) {
+          const int32_t s = nb[k] > (int32_t)c ? nb[k] : (int32_t)c;
+          const uint8_t st = p.cell_status[s];
+          const int32_t r = RING == 1 ? p.uf[s] : -1;
+          if (nb[k] > (int32_t)c && st != 0 && r != root_c) m |= 1u << k;
         }
-        if (!(box_box_d2(bb_c, p.bbox[nb]) <= eps_sq)) continue;
-        mask |= 1u << k;
+#pragma unroll
+        for (int k = 0; k < kPairsBatch; ++k) {
+          if (!((m >> k) & 1u)) continue;
+          if (!(box_box_d2(bb_c, p.bbox[nb[k]]) <= eps_sq)) m &= ~(1u << k);
+        }
+        mask |= m << h;
       }
     }
     // Warp-aggregated append of a variable number of pairs per lane.
@@ -286,10 +338,10 @@ __global__ void __launch_bounds__(256) k_pairs(Plan p, int ring, int skip_united
       if ((uint64_t)at + tot > (uint64_t)p.pair_cap) set_error(d, kErrCapacity);
     }
     at = __shfl_sync(kFull, at, 31) + x - cnt;
-    while (mask) {
-      const int k = __ffs(mask) - 1;
-      mask &= mask - 1;
-      if (at < p.pair_cap) p.plist[at] = make_int2((int32_t)c, row[kRingOffs[ring][k]]);
+#pragma unroll
+    for (int k = 0; k < nofs; ++k) {
+      if (!((mask >> k) & 1u)) continue;
+      if (at < p.pair_cap) p.plist[at] = make_int2((int32_t)c, row[kRingOffs[RING][k]]);
       ++at;
     }
   }
@@ -481,8 +533,12 @@ __global__ void __launch_bounds__(256) k_cid(Plan p) {
 // core items go first, so the whole grid sweeps the sorted points -- and the
 // input-order label writes of the clouds there -- together instead of
 // scattering them over the whole label array (3.5 ms against 7.6 ms for a
-// 151M-point, 4,096-cloud batch).
+// 151M-point, 4,096-cloud batch). With kGrouped (runs of up to kSmallRun
+// points) a border point loads the row entries, status, boxes and point
+// ranges of kNbGroupSmall neighbour cells together, and its core flag and
+// coordinates of each candidate together.
 
+template <bool kGrouped>
 __global__ void __launch_bounds__(kCellThreads) k_labels(Plan p) {
   const int64_t n = p.n;
   const int64_t bn = p.desc->b_count;
@@ -507,19 +563,55 @@ __global__ void __launch_bounds__(kCellThreads) k_labels(Plan p) {
       // its points are all strictly farther (point_box_d2 is a lower bound of
       // their rounded d2). A box at exactly the best d2 is still scanned, for
       // a tie with a smaller index.
-      for (int o = -1; o < kNgh - 1; ++o) {
-        const int32_t nb = row[o < 0 ? 12 : kNearFirst[o]];
-        if (nb < 0 || p.cell_status[nb] == 0) continue;
-        if (!(point_box_d2(q.x, q.y, p.bbox[nb]) <= best_d2)) continue;
-        const int32_t j1 = p.cell_start[nb + 1];
-        for (int32_t j = p.cell_start[nb]; j < j1; ++j) {
-          if (!p.is_core[j]) continue;
+      auto scan_cell = [&](int32_t nb, uint8_t st, float4 bb, int32_t j0, int32_t j1) {
+        if (nb < 0 || st == 0) return;
+        if (!(point_box_d2(q.x, q.y, bb) <= best_d2)) return;
+#pragma unroll 4
+        for (int32_t j = j0; j < j1; ++j) {
+          const uint8_t cj = p.is_core[j];
           const float2 pj = p.xy[j];
           const float d2 = sq_dist(__fsub_rn(pj.x, q.x), __fsub_rn(pj.y, q.y));
-          if (d2 <= eps_sq) {
+          if (cj && d2 <= eps_sq) {
             // d2 >= +0 and not NaN here, so its bits order like its value.
             const unsigned long long key = ((unsigned long long)__float_as_uint(d2) << 32) | p.perm[j];
             if (key < best) { best = key; best_nb = nb; best_d2 = d2; }
+          }
+        }
+      };
+      if constexpr (kGrouped) {
+        constexpr int G = kNbGroupSmall;
+        scan_cell(c, p.cell_status[c], p.bbox[c], p.cell_start[c], p.cell_start[c + 1]);
+        for (int g = 0; g < kNgh - 1; g += G) {
+          int32_t nb[G], j0[G], j1[G];
+          uint8_t st[G];
+          float4 bb[G];
+#pragma unroll
+          for (int u = 0; u < G; ++u) nb[u] = row[kNearFirst[g + u]];
+#pragma unroll
+          for (int u = 0; u < G; ++u) {
+            const int32_t s = max(nb[u], 0);  // cell 0 exists: this cloud has cell c
+            st[u] = p.cell_status[s];
+            bb[u] = p.bbox[s];
+            j0[u] = p.cell_start[s];
+            j1[u] = p.cell_start[s + 1];
+          }
+#pragma unroll
+          for (int u = 0; u < G; ++u) scan_cell(nb[u], st[u], bb[u], j0[u], j1[u]);
+        }
+      } else {
+        for (int o = -1; o < kNgh - 1; ++o) {
+          const int32_t nb = row[o < 0 ? 12 : kNearFirst[o]];
+          if (nb < 0 || p.cell_status[nb] == 0) continue;
+          if (!(point_box_d2(q.x, q.y, p.bbox[nb]) <= best_d2)) continue;
+          const int32_t j1 = p.cell_start[nb + 1];
+          for (int32_t j = p.cell_start[nb]; j < j1; ++j) {
+            if (!p.is_core[j]) continue;
+            const float2 pj = p.xy[j];
+            const float d2 = sq_dist(__fsub_rn(pj.x, q.x), __fsub_rn(pj.y, q.y));
+            if (d2 <= eps_sq) {
+              const unsigned long long key = ((unsigned long long)__float_as_uint(d2) << 32) | p.perm[j];
+              if (key < best) { best = key; best_nb = nb; best_d2 = d2; }
+            }
           }
         }
       }
@@ -535,7 +627,10 @@ __global__ void __launch_bounds__(kCellThreads) k_labels(Plan p) {
 
 // ------------------------------------------------------------- launchers
 cudaError_t launch_core(const Plan& p, cudaStream_t s) {
-  k_core<<<p.num_sms * p.bps[kTuneCore], kCellThreads, 0, s>>>(p);
+  if (p.n <= kSmallRun)
+    k_core<kNbGroupSmall><<<p.num_sms * p.bps[kTuneCore], kCellThreads, 0, s>>>(p);
+  else
+    k_core<kNbGroupLarge><<<p.num_sms * p.bps[kTuneCore], kCellThreads, 0, s>>>(p);
   k_status<<<p.num_sms * 8, 256, 0, s>>>(p);
   return cudaGetLastError();
 }
@@ -543,7 +638,10 @@ cudaError_t launch_core(const Plan& p, cudaStream_t s) {
 cudaError_t launch_union(const Plan& p, cudaStream_t s) {
   for (int ring = 0; ring < 2; ++ring) {
     if (ring == 1) k_flatten<<<p.num_sms * 8, 256, 0, s>>>(p);
-    k_pairs<<<p.num_sms * p.bps[kTunePairs], 256, 0, s>>>(p, ring, ring);
+    if (ring == 0)
+      k_pairs<0><<<p.num_sms * p.bps[kTunePairs], 256, 0, s>>>(p);
+    else
+      k_pairs<1><<<p.num_sms * p.bps[kTunePairs], 256, 0, s>>>(p);
     k_pair_scan<<<p.num_sms * p.bps[kTunePairScan], 256, 0, s>>>(p);
     k_pair_warp<<<p.num_sms * 8, 256, 0, s>>>(p);
   }
@@ -557,7 +655,10 @@ cudaError_t launch_ids(const Plan& p, cudaStream_t s) {
 
 cudaError_t launch_labels(const Plan& p, cudaStream_t s) {
   k_cid<<<p.num_sms * 4, 256, 0, s>>>(p);
-  k_labels<<<p.num_sms * p.bps[kTuneLabels], kCellThreads, 0, s>>>(p);
+  if (p.n <= kSmallRun)
+    k_labels<true><<<p.num_sms * p.bps[kTuneLabels], kCellThreads, 0, s>>>(p);
+  else
+    k_labels<false><<<p.num_sms * p.bps[kTuneLabels], kCellThreads, 0, s>>>(p);
   return cudaGetLastError();
 }
 
