@@ -261,6 +261,23 @@ __global__ void __launch_bounds__(kCellThreads, 5) k_cell_prep(Plan p) {
       if ((int)lane == l) p.bbox[c] = nan ? nan_box() : make_float4(xmin, xmax, ymin, ymax);
     }
 
+    // Query slots: a cell below ms points has all its points queried, a
+    // dense one none, so one scan of the lanes' query counts and one atomic
+    // per 32 cells place every query (in sorted order within the warp's
+    // cells), instead of a warp-aggregated atomic per 32 points whose
+    // returned base every later step of the walk would wait for.
+    const uint32_t nq = (valid && !huge && !dense) ? (uint32_t)(s1 - s0) : 0u;
+    uint32_t xq = nq;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(full, xq, o);
+      if (lane >= (uint32_t)o) xq += y;
+    }
+    const uint32_t totq = __shfl_sync(full, xq, 31);
+    uint32_t qbase = 0;
+    if (lane == 31 && totq) qbase = atomicAdd(&p.desc->q_count, totq);
+    const uint32_t qfirst = __shfl_sync(full, qbase, 31) + xq - nq;  // this cell's first slot
+
     // Points of the warp's cells, runs of consecutive non-huge cells at a
     // time (huge cells' points are classified by k_huge_bbox).
     uint32_t todo = __ballot_sync(full, valid && !huge);
@@ -281,11 +298,13 @@ __global__ void __launch_bounds__(kCellThreads, 5) k_cell_prep(Plan p) {
           if (sp <= i) lo += step;
         }
         const bool dn = __shfl_sync(full, dense, lo);
+        const int32_t cs0 = __shfl_sync(full, s0, lo);
+        const uint32_t cq = __shfl_sync(full, qfirst, lo);
         if (ok) {
           p.point_cell[i] = (int32_t)(wbase + lo);
           p.is_core[i] = dn ? 1 : 0;
+          if (!dn) p.qlist[cq + (uint32_t)(i - cs0)] = (uint32_t)i;
         }
-        append_list(p.qlist, &p.desc->q_count, ok && !dn, (uint32_t)i);
       }
     }
 
@@ -376,6 +395,8 @@ __global__ void __launch_bounds__(kCellThreads, 5) k_cell_prep(Plan p) {
 // any huge cell, reduces the chunk, and the warp that finishes a cell's last
 // chunk folds the cell's chunk boxes into bbox[c]. Min and max are
 // order-independent, so the box equals the reference's serial fold.
+constexpr int kHugeBatch = 8;  // loads a warp of k_huge_bbox keeps in flight
+
 __global__ void __launch_bounds__(256) k_huge_bbox(Plan p) {
   const uint32_t full = 0xffffffffu;
   const uint32_t lane = lane_id();
@@ -403,20 +424,31 @@ __global__ void __launch_bounds__(256) k_huge_bbox(Plan p) {
     // The chunk's points also get their cell and class, as k_cell_prep gives
     // every other point (a huge cell is below ms only when ms > kHugeCell).
     const bool dn = (s1 - s0) >= p.seg_param[p.cell_seg[c]].ms;
-    for (int32_t base = a; base < b; base += 32) {
-      const int32_t i = base + (int32_t)lane;
-      const bool ok = i < b;
-      if (ok) {
-        p.point_cell[i] = c;
-        p.is_core[i] = dn ? 1 : 0;
-        const float2 v = p.xy[i];
-        if (isnan(v.x) || isnan(v.y)) {  // whole box becomes nan_box()
-          xmin = -INFINITY; xmax = INFINITY; ymin = -INFINITY; ymax = INFINITY;
-        }
-        xmin = fminf(xmin, v.x); xmax = fmaxf(xmax, v.x);
-        ymin = fminf(ymin, v.y); ymax = fmaxf(ymax, v.y);
+    // kHugeBatch steps of 32 points have their loads in flight together.
+    for (int32_t base0 = a; base0 < b; base0 += 32 * kHugeBatch) {
+      float2 v[kHugeBatch];
+#pragma unroll
+      for (int u = 0; u < kHugeBatch; ++u) {
+        const int32_t i = base0 + 32 * u + (int32_t)lane;
+        v[u] = i < b ? p.xy[i] : make_float2(0.f, 0.f);
       }
-      append_list(p.qlist, &d->q_count, ok && !dn, (uint32_t)i);
+#pragma unroll
+      for (int u = 0; u < kHugeBatch; ++u) {
+        const int32_t base = base0 + 32 * u;
+        if (base >= b) break;  // warp-uniform
+        const int32_t i = base + (int32_t)lane;
+        const bool ok = i < b;
+        if (ok) {
+          p.point_cell[i] = c;
+          p.is_core[i] = dn ? 1 : 0;
+          if (isnan(v[u].x) || isnan(v[u].y)) {  // whole box becomes nan_box()
+            xmin = -INFINITY; xmax = INFINITY; ymin = -INFINITY; ymax = INFINITY;
+          }
+          xmin = fminf(xmin, v[u].x); xmax = fmaxf(xmax, v[u].x);
+          ymin = fminf(ymin, v[u].y); ymax = fmaxf(ymax, v[u].y);
+        }
+        append_list(p.qlist, &d->q_count, ok && !dn, (uint32_t)i);
+      }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -436,10 +468,19 @@ __global__ void __launch_bounds__(256) k_huge_bbox(Plan p) {
       __threadfence();
       const int64_t b0 = (int64_t)p.big_base[lo];
       xmin = INFINITY; xmax = -INFINITY; ymin = INFINITY; ymax = -INFINITY;
-      for (int32_t t = lane; t < nch; t += 32) {
-        const float4 v = __ldcg(&p.big_chunk_box[b0 + t]);
-        xmin = fminf(xmin, v.x); xmax = fmaxf(xmax, v.y);
-        ymin = fminf(ymin, v.z); ymax = fmaxf(ymax, v.w);
+      for (int32_t t0 = lane; t0 < nch; t0 += 32 * kHugeBatch) {
+        float4 v[kHugeBatch];
+#pragma unroll
+        for (int u = 0; u < kHugeBatch; ++u) {
+          const int32_t t = t0 + 32 * u;
+          v[u] = t < nch ? __ldcg(&p.big_chunk_box[b0 + t])
+                         : make_float4(INFINITY, -INFINITY, INFINITY, -INFINITY);
+        }
+#pragma unroll
+        for (int u = 0; u < kHugeBatch; ++u) {
+          xmin = fminf(xmin, v[u].x); xmax = fmaxf(xmax, v[u].y);
+          ymin = fminf(ymin, v[u].z); ymax = fmaxf(ymax, v[u].w);
+        }
       }
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) {

@@ -617,9 +617,15 @@ __global__ void __launch_bounds__(kCellThreads) k_labels(Plan p) {
       }
       lab = best_nb < 0 ? -1 : p.cid[best_nb];
     } else {
+      // Core flag, cell and destination loaded together (nearly every point
+      // here is core), so the label waits for two memory latencies, not four.
       i = core_first ? t : t - bn;
-      if (!p.is_core[i]) continue;
-      lab = p.cid[p.point_cell[i]];
+      const uint8_t core = p.is_core[i];
+      const int32_t cell = p.point_cell[i];
+      const uint32_t dst = p.perm[i];
+      if (!core) continue;
+      p.labels[dst] = p.cid[cell];
+      continue;
     }
     p.labels[p.perm[i]] = lab;
   }
