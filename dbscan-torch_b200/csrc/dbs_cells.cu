@@ -191,23 +191,64 @@ __device__ __forceinline__ void append_list(uint32_t* list, uint32_t* count, boo
 //     coalesced;
 //   - the 25-entry neighbour row of each cell, staged in shared memory and
 //     written as one contiguous block per warp.
+//
+// LPC lanes per cell (32 / LPC cells per warp): with LPC > 1 (runs of up to
+// kSmallRun points) the lanes of a cell split its box fold and its five
+// neighbour columns, so a small cloud has LPC times as many warps of work.
+// A 1M-point cloud has about 64k cells: 2,016 warps of 32 cells for 148
+// SMs left 9.7 warps per SM active.
+template <int LPC>
 __global__ void __launch_bounds__(kCellThreads, 5) k_cell_prep(Plan p) {
-  __shared__ int32_t s_row[kCellThreads / 32][32 * kNgh];
+  static_assert(LPC == 1 || LPC == 2 || LPC == 4, "lanes per cell");
+  constexpr int CPW = 32 / LPC;  // cells per warp
+  __shared__ int32_t s_row[kCellThreads / 32][CPW * kNgh];
   const uint32_t full = 0xffffffffu;
   const uint32_t lane = lane_id();
+  const uint32_t sub = lane % LPC;   // this lane's part of its cell
+  const uint32_t cl = lane / LPC;    // this lane's cell within the warp
+  const int lead = (int)(lane - sub);  // first lane of the cell
   int32_t* srow = s_row[threadIdx.x >> 5];
   const uint32_t C = p.desc->num_cells;
   const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-  for (uint32_t wbase = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; wbase < C;
-       wbase += warps * 32) {
-    const uint32_t c = wbase + lane;
+  for (uint32_t wbase = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * CPW; wbase < C;
+       wbase += warps * CPW) {
+    const uint32_t c = wbase + cl;
     const bool valid = c < C;
     int32_t s0 = INT32_MAX, s1 = INT32_MAX, seg = 0;
     if (valid) { s0 = p.cell_start[c]; s1 = p.cell_start[c + 1]; seg = p.cell_seg[c]; }
     const bool big = valid && (s1 - s0) > kBigCell;
     const bool huge = big && (s1 - s0) > kHugeCell;
     const bool dense = valid && (s1 - s0) >= p.seg_param[seg].ms;
-    if (valid && !big) {
+    if constexpr (LPC > 1) {
+      // Each lane of the cell folds every LPC-th point (fminf/fmaxf flush
+      // subnormals, as the reference's fold does), then the lanes combine.
+      const bool fold = valid && !big;
+      float4 b = make_float4(INFINITY, -INFINITY, INFINITY, -INFINITY);
+      bool nan = false;
+      if (fold) {
+        for (int32_t i = s0 + (int32_t)sub; i < s1; i += LPC) {
+          const float2 v = p.xy[i];
+          nan |= isnan(v.x) || isnan(v.y);
+          b.x = fminf(b.x, v.x); b.y = fmaxf(b.y, v.x);
+          b.z = fminf(b.z, v.y); b.w = fmaxf(b.w, v.y);
+        }
+      }
+#pragma unroll
+      for (int o = 1; o < LPC; o <<= 1) {
+        b.x = fminf(b.x, __shfl_xor_sync(full, b.x, o));
+        b.y = fmaxf(b.y, __shfl_xor_sync(full, b.y, o));
+        b.z = fminf(b.z, __shfl_xor_sync(full, b.z, o));
+        b.w = fmaxf(b.w, __shfl_xor_sync(full, b.w, o));
+        nan |= __shfl_xor_sync(full, nan ? 1 : 0, o) != 0;
+      }
+      if (fold && sub == 0) {
+        if (s1 - s0 == 1) {  // raw coordinates, as below
+          const float2 v = p.xy[s0];
+          b = make_float4(v.x, v.x, v.y, v.y);
+        }
+        p.bbox[c] = nan ? nan_box() : b;
+      }
+    } else if (valid && !big) {
       // Fold the box. A one-point cell keeps its raw coordinates: the
       // reference seeds the fold with xs[s] and flushes subnormals only
       // through fminf/fmaxf.
@@ -226,7 +267,7 @@ __global__ void __launch_bounds__(kCellThreads, 5) k_cell_prep(Plan p) {
       }
       p.bbox[c] = nan ? nan_box() : b;
     }
-    if (huge) {
+    if (huge && sub == 0) {
       // Registered for k_huge_bbox: one entry, ceil(size / kHugeChunk) chunks.
       const unsigned long long nch = (unsigned long long)((s1 - s0 + kHugeChunk - 1) / kHugeChunk);
       const unsigned long long old = atomicAdd(&p.desc->big_packed, (1ull << 40) + nch);
@@ -237,7 +278,7 @@ __global__ void __launch_bounds__(kCellThreads, 5) k_cell_prep(Plan p) {
         p.big_done[e] = 0;
       }
     }
-    uint32_t bm = __ballot_sync(full, big && !huge);
+    uint32_t bm = __ballot_sync(full, big && !huge && sub == 0);
     while (bm) {
       const int l = __ffs(bm) - 1;
       bm &= bm - 1;
@@ -266,7 +307,7 @@ __global__ void __launch_bounds__(kCellThreads, 5) k_cell_prep(Plan p) {
     // per 32 cells place every query (in sorted order within the warp's
     // cells), instead of a warp-aggregated atomic per 32 points whose
     // returned base every later step of the walk would wait for.
-    const uint32_t nq = (valid && !huge && !dense) ? (uint32_t)(s1 - s0) : 0u;
+    const uint32_t nq = (valid && !huge && !dense && sub == 0) ? (uint32_t)(s1 - s0) : 0u;
     uint32_t xq = nq;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -276,7 +317,8 @@ __global__ void __launch_bounds__(kCellThreads, 5) k_cell_prep(Plan p) {
     const uint32_t totq = __shfl_sync(full, xq, 31);
     uint32_t qbase = 0;
     if (lane == 31 && totq) qbase = atomicAdd(&p.desc->q_count, totq);
-    const uint32_t qfirst = __shfl_sync(full, qbase, 31) + xq - nq;  // this cell's first slot
+    uint32_t qfirst = __shfl_sync(full, qbase, 31) + xq - nq;  // this cell's first slot
+    if constexpr (LPC > 1) qfirst = __shfl_sync(full, qfirst, lead);
 
     // Points of the warp's cells, runs of consecutive non-huge cells at a
     // time (huge cells' points are classified by k_huge_bbox).
@@ -301,7 +343,7 @@ __global__ void __launch_bounds__(kCellThreads, 5) k_cell_prep(Plan p) {
         const int32_t cs0 = __shfl_sync(full, s0, lo);
         const uint32_t cq = __shfl_sync(full, qfirst, lo);
         if (ok) {
-          p.point_cell[i] = (int32_t)(wbase + lo);
+          p.point_cell[i] = (int32_t)(wbase + lo / LPC);
           p.is_core[i] = dn ? 1 : 0;
           if (!dn) p.qlist[cq + (uint32_t)(i - cs0)] = (uint32_t)i;
         }
@@ -321,7 +363,18 @@ __global__ void __launch_bounds__(kCellThreads, 5) k_cell_prep(Plan p) {
 #pragma unroll
       for (int dy = 0; dy < 5; ++dy)
         ngy[dy] = compact_axis((int32_t)((uint32_t)ky + (uint32_t)(dy - 2)), g.by, g.py);
-      if (g.map_base >= 0) {
+      if (g.map_base >= 0 && LPC > 1) {
+        // Dense cloud: this lane's map rows (every LPC-th column).
+#pragma unroll
+        for (int dx = 0; dx < 5; ++dx) {
+          if (dx % LPC != (int)sub) continue;
+          const uint64_t ngx = compact_axis((int32_t)((uint32_t)kx + (uint32_t)(dx - 2)), g.bx, g.px);
+          const int32_t* mrow = p.cell_map + g.map_base + (int64_t)(ngx * g.ys);
+#pragma unroll
+          for (int dy = 0; dy < 5; ++dy)
+            srow[cl * kNgh + dx * 5 + dy] = (ngx != ~0ull && ngy[dy] != ~0ull) ? mrow[ngy[dy]] : -1;
+        }
+      } else if (g.map_base >= 0) {
         // Dense cloud: five map rows, 25 independent loads.
         int32_t r[25];
 #pragma unroll
@@ -333,7 +386,7 @@ __global__ void __launch_bounds__(kCellThreads, 5) k_cell_prep(Plan p) {
             r[dx * 5 + dy] = (ngx != ~0ull && ngy[dy] != ~0ull) ? mrow[ngy[dy]] : -1;
         }
 #pragma unroll
-        for (int k = 0; k < 25; ++k) srow[lane * kNgh + k] = r[k];
+        for (int k = 0; k < 25; ++k) srow[cl * kNgh + k] = r[k];
       } else {
         // Sparse cloud: its cells are sorted by key, and the five neighbours
         // of one column (same gx) are the keys base + ngx * ys + ngy[dy].
@@ -359,7 +412,8 @@ __global__ void __launch_bounds__(kCellThreads, 5) k_cell_prep(Plan p) {
         const int64_t lo0 = g.cell_begin, hi0 = min((int64_t)C, lo0 + npts);
 #pragma unroll
         for (int dx = 0; dx < 5; ++dx) {
-          int32_t* out = srow + lane * kNgh + dx * 5;
+          if (dx % LPC != (int)sub) continue;  // another lane's column
+          int32_t* out = srow + cl * kNgh + dx * 5;
           const uint64_t ngx = compact_axis((int32_t)((uint32_t)kx + (uint32_t)(dx - 2)), g.bx, g.px);
           if (ngx == ~0ull || sy[0] == ~0ull) {
 #pragma unroll
@@ -383,7 +437,7 @@ __global__ void __launch_bounds__(kCellThreads, 5) k_cell_prep(Plan p) {
       }
     }
     __syncwarp();
-    const int32_t rows = (int32_t)min(32u, C - wbase);
+    const int32_t rows = (int32_t)min((uint32_t)CPW, C - wbase);
     int32_t* out = p.ngh + (int64_t)wbase * kNgh;
     for (int32_t k = (int32_t)lane; k < rows * kNgh; k += 32) out[k] = srow[k];
     __syncwarp();
@@ -503,7 +557,10 @@ cudaError_t launch_rle(const Plan& p, cudaStream_t s) {
 }
 
 cudaError_t launch_cell_prep(const Plan& p, cudaStream_t s) {
-  k_cell_prep<<<p.num_sms * p.bps[kTuneCellPrep], kCellThreads, 0, s>>>(p);
+  if (p.n <= kSmallRun)
+    k_cell_prep<4><<<p.num_sms * p.bps[kTuneCellPrep], kCellThreads, 0, s>>>(p);
+  else
+    k_cell_prep<1><<<p.num_sms * p.bps[kTuneCellPrep], kCellThreads, 0, s>>>(p);
   k_huge_bbox<<<p.num_sms * 4, 256, 0, s>>>(p);
   return cudaGetLastError();
 }

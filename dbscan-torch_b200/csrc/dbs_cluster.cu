@@ -54,7 +54,6 @@ __constant__ int8_t kNearFirst[24] = {7, 11, 13, 17, 6, 8, 16, 18, 2, 10, 14, 22
 // 12.6 and 23.2 -> 13.3 us; 10M points, k_core 76.3 -> 71.0 us (groups of
 // 2), while groups of 4 (46 and 58 registers) slowed k_core to 87.7 us and
 // k_labels from 111.2 to 150.3 us.
-constexpr int64_t kSmallRun = 2 << 20;
 constexpr int kNbGroupSmall = 4;
 constexpr int kNbGroupLarge = 2;
 

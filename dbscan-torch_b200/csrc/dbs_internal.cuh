@@ -84,8 +84,16 @@ enum : int {
   kTuneLabels,
   kNumTuned
 };
-constexpr int32_t kDefaultBlocksPerSm[kNumTuned] = {8, 8, 8, 8, 8, 8};
+// The count kernel's launch bounds let 6 blocks per SM be resident; a grid of
+// exactly those (no second partial wave) measured 76.0 -> 71.8 us at 10M
+// points and 456 -> 349 us on a 1,024-cloud batch. The cell pass keeps 8 (5
+// are resident) though: 5 measured 106.9 -> 121.7 us at 10M points.
+constexpr int32_t kDefaultBlocksPerSm[kNumTuned] = {6, 8, 8, 8, 8, 8};
 constexpr int32_t kLabelsBlocksPerSmBorderFirst = 32;
+// Runs of up to this many points take the latency-bound forms of the cell,
+// core and label passes (wider groups of independent loads, several lanes
+// per cell); larger runs take the forms that keep more warps resident.
+constexpr int64_t kSmallRun = 2 << 20;
 // Label pass item order: border items first up to this many points (labels
 // that fit L2), core items first above (k_labels).
 constexpr int64_t kCoreFirstPoints = 16 << 20;

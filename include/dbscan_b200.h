@@ -134,7 +134,8 @@ typedef struct dbs_launch_shape {
 } dbs_launch_shape;
 
 /* The built-in shape of a run over n_total points (every entry non-zero):
- * 8 blocks per SM; the label pass 32 up to 2^24 points, 8 above. */
+ * the per-key count 6 blocks per SM (the blocks resident at once), the label
+ * pass 32 up to 2^24 points and 8 above, every other kernel 8. */
 int dbs_default_launch_shape(int64_t n_total, dbs_launch_shape* out);
 
 /* dbs_dbscan2d_batched_device with a launch shape (NULL = built-in). An entry

@@ -61,9 +61,9 @@ def test_capi_shape_checks():
     sh = _Shape()
     lib.dbs_default_launch_shape.argtypes = [ctypes.c_int64, ctypes.c_void_p]
     assert lib.dbs_default_launch_shape(10_000_000, ctypes.byref(sh)) == 0
-    assert list(sh.blocks_per_sm) == [8, 8, 8, 8, 8, 32]
+    assert list(sh.blocks_per_sm) == [6, 8, 8, 8, 8, 32]
     assert lib.dbs_default_launch_shape((16 << 20) + 1, ctypes.byref(sh)) == 0
-    assert list(sh.blocks_per_sm) == [8] * 6
+    assert list(sh.blocks_per_sm) == [6, 8, 8, 8, 8, 8]
     assert lib.dbs_default_launch_shape(10, None) == 1
     assert lib.dbs_default_launch_shape(-1, ctypes.byref(sh)) == 1
     f = lib.dbs_dbscan2d_batched_device_shaped
