@@ -659,7 +659,10 @@ static int grid_for(const Plan& p, int64_t work, int threads, int per_sm) {
 cudaError_t launch_front(const Plan& p, cudaStream_t s) {
   k_init<<<grid_for(p, (int64_t)p.nseg + p.ids_tiles + 2 * kRadix, 256, 2), 256, 0, s>>>(p);
   k_bounds<<<grid_for(p, p.n, 256 * 8, 8), 256, 0, s>>>(p);
-  k_seg_finalize<<<1, 1024, 0, s>>>(p);
+  // One block; its scans take log2(threads) rounds of block barriers, so a
+  // call with few clouds takes a small block (one warp for a plain call).
+  const int fin_threads = p.nseg <= 32 ? 32 : (p.nseg <= 256 ? 256 : 1024);
+  k_seg_finalize<<<1, fin_threads, 0, s>>>(p);
   return cudaGetLastError();
 }
 
